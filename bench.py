@@ -1,0 +1,380 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the dense acoustic FDTD step on B200.
+
+Workload: the 512x384x256 room (50.3M cells; Ricker 1 kHz point source at a
+seeded interior cell, 8 seeded receivers, per-face absorption ~ U[0.02, 0.3],
+reference time step).  One bench step = one FDTD time step over the whole grid
+(velocity + pressure update, source deposit, 8 receiver samples).
+
+Lines printed (rank 0, one JSON object):
+  value     Gcell-updates/s with fields resident in HBM (async stepping,
+            CUDA events on the solver's stream, max over ranks);
+  e2e       the same metric through the reference-facing C ABI with host
+            buffers, per step: fdtd_b200_add_pressure (source sample from the
+            host), fdtd_step(st, 1), fdtd_sample_pressure_precomputed (host
+            sampler arrays in, 8 receiver values out);
+  roofline  the fused step kernel: 32 algorithmic bytes per cell-update over
+            its mean launch duration (CUDA events around every launch on the
+            launching stream) against the measured HBM copy bandwidth;
+  cpu_baseline  the reference's own CPU solver (oracle/_ref, its std::thread
+            pool over all host cores) on a time-bounded sample of the same room.
+
+--impl reference times the reference's CPU solver alone (rank 0; other ranks
+exit 0).  Multi-GPU (torchrun): every rank advances its own copy of the room
+(independent replicas, weak scaling); value sums the ranks' cells over the
+slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL_UPDATE = 32          # read + write of p, vx, vy, vz in float32
+METRIC = "Gcell-updates/s"
+PEAKS_FILE = os.path.join(ROOT, "MEASURED_PEAKS.json")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "fused_step_room512x384x256.md")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3000)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    ap.add_argument("--kernel", choices=["auto", "fused", "two_pass"], default="auto")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0,
+                    help="bound on the CPU-baseline sample")
+    ap.add_argument("--ref-seconds", type=float, default=90.0,
+                    help="bound on the timed part of --impl reference")
+    return ap.parse_args()
+
+
+def workload():
+    from spectral_analyzer_b200.rooms import large_room
+    return large_room(n_steps=10000)
+
+
+def config_dict(room, n, kernel):
+    return {"workload": "room512x384x256_ricker_8rec", "grid": [room.nx, room.ny, room.nz],
+            "cells": room.cells, "receivers": len(room.receivers), "source": "ricker_1kHz",
+            "absorption": [round(a, 6) for a in room.absorption], "n_pml": room.n_pml,
+            "dt_s": room.dt, "courant": 0.77 / 3 ** 0.5, "step_kernel": kernel,
+            "parallelism": f"replicas{n}" if n > 1 else "single",
+            "l2_flush": "none: working set 1.6 GB (P x2, V x2 sets) exceeds the 126 MB L2"}
+
+
+def measured_peak():
+    try:
+        with open(PEAKS_FILE) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic_per_launch():
+    """DRAM bytes per fused-step launch from the committed ncu summary, if present."""
+    try:
+        with open(TRAFFIC_FILE) as f:
+            for line in f:
+                if line.startswith("dram_bytes_per_launch_full_room:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id: str):
+        self.gpu_id = gpu_id
+        self.proc = None
+        self.path = os.path.join("/tmp", f"fdtd_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", self.gpu_id, f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.fh, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.fh.close()
+
+    def summary(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[4:]))
+                except ValueError:
+                    continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        loaded = [r for r in rows if r[2] > 250.0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[q] for r in loaded for q, v in enumerate(r[3][1:5]) if v.lower() == "active"})
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows), "samples_under_load": len(loaded),
+                "power_w_max": max(r[2] for r in rows)}
+
+
+def cpu_baseline(room, seconds: float):
+    """The reference's own solver on the same room, time-bounded; Gcell-updates/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    if orc.reference_available():
+        f = orc.RefFDTD(room.nx, room.ny, room.nz, room.dx, room.c, room.rho, n_pml=room.n_pml,
+                        fast=True)
+        f.set_face_absorption(room.absorption)
+        kind, cores = "reference", orc.RefFDTD.pool_threads()
+        lib = os.path.basename(f.library_path)
+    else:
+        f = orc.OracleFDTD(room.nx, room.ny, room.nz, room.dx, room.c, room.rho, n_pml=room.n_pml)
+        f.set_face_absorption(room.absorption)
+        kind, cores, lib = "port", 1, "liboracle_fdtd.so"
+    idx, w = f.precompute_pressure_samplers(room.receiver_xyz())
+    sig = room.signal()
+    f.add_pressure(room.src_flat, float(sig[0]))
+    f.step(1)                                   # untimed first step (page-in)
+    n = 0
+    t0 = time.perf_counter()
+    while True:
+        sc = f.step_count
+        f.add_pressure(room.src_flat, float(sig[sc]))
+        f.step(1)
+        f.sample_pressure_precomputed(idx, w)
+        n += 1
+        el = time.perf_counter() - t0
+        if el >= seconds or n >= 400:
+            break
+    del f
+    val = room.cells * n / el / 1e9
+    return {"value": val, "unit": METRIC, "cores": cores, "kind": kind,
+            "sample": f"{n} steps of the 512x384x256 room after 1 warm-up step ({el:.1f} s wall, "
+                      f"{lib}, source deposit + step + 8-receiver sample per step)"}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    room = workload()
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as orc
+    if orc.reference_available():
+        f = orc.RefFDTD(room.nx, room.ny, room.nz, room.dx, room.c, room.rho, n_pml=room.n_pml,
+                        fast=True)
+        kind, cores, lib = "reference", orc.RefFDTD.pool_threads(), None
+        lib = os.path.basename(f.library_path)
+    else:
+        f = orc.OracleFDTD(room.nx, room.ny, room.nz, room.dx, room.c, room.rho, n_pml=room.n_pml)
+        kind, cores, lib = "port", 1, "liboracle_fdtd.so"
+    f.set_face_absorption(room.absorption)
+    idx, w = f.precompute_pressure_samplers(room.receiver_xyz())
+    sig = room.signal()
+
+    def one():
+        f.add_pressure(room.src_flat, float(sig[f.step_count]))
+        f.step(1)
+        f.sample_pressure_precomputed(idx, w)
+
+    for _ in range(min(args.warmup, 2)):
+        one()
+    n = 0
+    t0 = time.perf_counter()
+    while n < args.steps:
+        one()
+        n += 1
+        if time.perf_counter() - t0 >= args.ref_seconds:
+            break
+    el = time.perf_counter() - t0
+    val = room.cells * n / el / 1e9
+    sample = (f"{n} of {args.steps} requested steps of the 512x384x256 room (time-bounded at "
+              f"{args.ref_seconds:.0f} s) after {min(args.warmup, 2)} warm-up steps, {lib}")
+    line = {"impl": "reference", "metric": METRIC, "value": val, "unit": METRIC, "n_gpus": args.gpus,
+            "steps": n, "warmup": min(args.warmup, 2), "ms_per_step": el / n * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config_dict(room, 1, "reference_cpu"),
+            "cpu_baseline": {"value": val, "unit": METRIC, "cores": cores, "kind": kind,
+                             "sample": sample},
+            "e2e": {"value": val, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def engine_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from spectral_analyzer_b200 import AcousticFDTD, _native
+
+    room = workload()
+    f = AcousticFDTD(room.nx, room.ny, room.nz, room.dx, room.c, room.rho,
+                     cell_type=room.cell_type(), plate_iz=-1, plate_active=room.plate_active(),
+                     n_pml=room.n_pml)
+    f.set_face_absorption(room.absorption)
+    f.set_kernel(args.kernel)
+    kernel = f.kernel
+    idx8, wgt8 = f.precompute_pressure_samplers(room.receiver_xyz())
+    sig = room.signal()
+    K, W = args.steps, args.warmup
+    f.set_point_source(room.src_flat, sig)
+    f.set_receivers(idx8, wgt8, capacity=K + W)
+    stream = f.torch_stream()          # the stream every solver kernel is launched on
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ---- device-resident throughput ----
+    f.step_async(W)
+    assert f.synchronize() == 0
+    gpu_id = str(torch.cuda.get_device_properties(local).uuid)
+    gpu_id = gpu_id if gpu_id.startswith("GPU-") else "GPU-" + gpu_id
+    f.profile(True)
+    launches0 = f.launch_count
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_id) as clk:
+        e0.record(stream)
+        rc = f.step_async(K)
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = f.launch_count - launches0
+    assert rc == 0 and f.synchronize() == 0, "instability during the timed run"
+    ms = e0.elapsed_time(e1)
+    prof_ms, prof_n, _ = f.profile_read()
+    f.profile(False)
+    t_max = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t_max, op=dist.ReduceOp.MAX)
+    ms_max = float(t_max.item())
+    traces = f.get_traces()
+    assert traces.shape == (K + W, len(room.receivers))
+    assert np.isfinite(traces).all()
+
+    value = room.cells * K * world / (ms_max / 1e3) / 1e9
+    kern_ms = prof_ms / max(prof_n, 1)
+    achieved = BYTES_PER_CELL_UPDATE * room.cells / (kern_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    traffic = ncu_traffic_per_launch()
+
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = None
+    if not args.no_e2e:
+        import ctypes as C
+        lib = _native.load()
+        h = f._h
+        f.set_point_source(room.src_flat, None)
+        f.set_receivers(np.zeros(0, np.int32), np.zeros(0, np.float32), 0)
+        idx_c = np.ascontiguousarray(idx8, np.int32)
+        w_c = np.ascontiguousarray(wgt8, np.float32)
+        out = np.zeros(len(room.receivers), np.float32)
+        p_idx, p_w, p_out = (idx_c.ctypes.data_as(_native.P_i32), w_c.ctypes.data_as(_native.P_f32),
+                             out.ctypes.data_as(_native.P_f32))
+        n_rec = len(room.receivers)
+        src = room.src_flat
+
+        def e2e_step(n):
+            lib.fdtd_b200_add_pressure(h, src, float(sig[n % len(sig)]))
+            rc_ = lib.fdtd_step(h, 1)
+            rc2 = lib.fdtd_sample_pressure_precomputed(h, n_rec, p_idx, p_w, p_out)
+            return rc_ | rc2
+
+        for n in range(W):
+            e2e_step(n)
+        barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        bad = 0
+        for n in range(K):
+            bad |= e2e_step(n)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        t2 = torch.tensor([el], dtype=torch.float64, device="cuda")
+        if world > 1:
+            dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+        el = float(t2.item())
+        assert bad == 0
+        e2e = {"value": room.cells * K * world / el / 1e9, "unit": METRIC,
+               "h2d_bytes_per_step": 4 + n_rec * 8 * (8 + 4), "d2h_bytes_per_step": n_rec * 4,
+               "ms_per_step": el / K * 1e3,
+               "path": "fdtd_b200_add_pressure + fdtd_step(st,1) + fdtd_sample_pressure_precomputed"}
+
+    f.close()
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(room, args.cpu_seconds)
+
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": METRIC, "n_gpus": world, "steps": K,
+                "warmup": W, "ms_per_step": ms_max / K, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config_dict(room, world, kernel),
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic,
+                             "peak_kind": f"{peak_kind} hbm_gbs",
+                             "kernel": "k_fused_step" if kernel == "fused" else "k_velocity_general+k_pressure_general",
+                             "kernel_ms_mean": kern_ms, "kernel_launches_timed": prof_n,
+                             "algorithmic_bytes_per_launch": BYTES_PER_CELL_UPDATE * room.cells},
+                "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": launches,
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return engine_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

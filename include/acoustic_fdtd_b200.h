@@ -1,0 +1,242 @@
+/*
+ * acoustic_fdtd_b200.h — C ABI of the B200 (sm_100a) acoustic FDTD engine.
+ *
+ * Drop-in for the reference's csrc/include/acoustic_fdtd.h
+ * (sangderenard/spectral-analyzer): the 26 fdtd_* entry points below keep the
+ * reference's names, signatures, argument meaning, array layouts and return
+ * codes, so a caller of that header (the pybind AcousticFDTD wrapper,
+ * csrc/bindings/pybind_kernels.cpp:5473-5664, or the uniform co-evolver,
+ * csrc/kernels/acoustic_coevolver.cpp:1015-2205) relinks against
+ * libacoustic_fdtd_b200.so unchanged.  The fields live in GPU memory; every
+ * host array crossing this ABI is caller-owned and copied.
+ *
+ * Physics and numerics are the reference's: staggered p/Vx/Vy/Vz leapfrog,
+ * 4th-order interior gradient and divergence, cubic-graded PML, rigid walls,
+ * cut-cell face fractions, Kirchhoff plate.  In float32 the engine rounds
+ * exactly like the reference compiled without FMA contraction, so fields,
+ * traces and return codes are bit-identical.
+ *
+ * Layouts seen through this ABI are the reference's (acoustic_fdtd.h:67-71,
+ * :430-437): P index k + Nz*(j + Ny*i); Vx k + Nz*(j + Ny*i) for i < Nx-1;
+ * Vy k + Nz*(j + (Ny-1)*i); Vz k + (Nz-1)*(j + Ny*i).  On the device every field
+ * is stored padded as [Nx][Ny][Sz] with Sz = Nz rounded up to a multiple of 8
+ * (fdtd_b200_field_layout).
+ *
+ * Threading: a handle is not thread-safe (as in the reference).  Calls that
+ * return data or a status synchronise the handle's stream before returning;
+ * fdtd_step synchronises only when a stability check or the plate guard runs
+ * inside the call (every 256 steps, or every step while a plate is active).
+ *
+ * Codes: FDTD_OK 0, FDTD_ERR_NULL -1, FDTD_ERR_DIM -2, FDTD_ERR_UNSTABLE -3 as
+ * in the reference; the engine adds FDTD_ERR_CUDA -4 (CUDA runtime failure;
+ * fdtd_b200_last_error has the text) and FDTD_ERR_ARG -5 (invalid argument to
+ * an extension, or an out-of-range index that the reference would have read
+ * out of bounds).
+ */
+#pragma once
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDTD_B200_API __attribute__((visibility("default")))
+
+#define FDTD_AIR   ((uint8_t)0)
+#define FDTD_WALL  ((uint8_t)1)
+#define FDTD_PLATE ((uint8_t)2)
+#define FDTD_PML   ((uint8_t)3)
+
+#define FDTD_OK            0
+#define FDTD_ERR_NULL     (-1)
+#define FDTD_ERR_DIM      (-2)
+#define FDTD_ERR_UNSTABLE (-3)
+#define FDTD_ERR_CUDA     (-4)
+#define FDTD_ERR_ARG      (-5)
+
+typedef struct AcousticFDTDState AcousticFDTDState;
+
+/* ===================== reference entry points (acoustic_fdtd.h) ===================== */
+
+/* acoustic_fdtd.h:137-152.  Builds the solver on the current CUDA device and
+ * allocates its fields there.  NULL on invalid arguments, when no CUDA device
+ * is usable, or when device memory runs out. */
+FDTD_B200_API AcousticFDTDState* fdtd_create(
+    int Nx, int Ny, int Nz, float dx, float c, float rho_air,
+    const uint8_t* cell_type, int plate_iz, const uint8_t* plate_active,
+    float plate_mass_density, float plate_stiffness_D,
+    float plate_alpha_M, float plate_beta_K, int n_pml);
+
+/* acoustic_fdtd.h:155. */
+FDTD_B200_API void fdtd_destroy(AcousticFDTDState* st);
+
+/* acoustic_fdtd.h:171-175.  Weights normalised by the sum of |w|. */
+FDTD_B200_API int fdtd_set_bridge_sources(AcousticFDTDState* st, int n_cells,
+                                          const int* cell_indices, const float* weights);
+
+/* acoustic_fdtd.h:184-188.  Disabled in the reference; returns FDTD_ERR_UNSTABLE. */
+FDTD_B200_API int fdtd_inject_bridge(AcousticFDTDState* st, float signal_val,
+                                     float signal_ddt, float force_scale);
+
+/* acoustic_fdtd.h:206-209.  Accumulates into the plate load consumed by the next step. */
+FDTD_B200_API int fdtd_inject_bridge_drive(AcousticFDTDState* st, const float* cell_drives,
+                                           float force_scale);
+
+/* acoustic_fdtd.h:219-224. */
+FDTD_B200_API int fdtd_inject_plate_force(AcousticFDTDState* st, int n_plate,
+                                          const int* plate_indices, const float* weights,
+                                          float total_force_N);
+
+/* acoustic_fdtd.h:246-250.  NULL leaves a component unchanged. */
+FDTD_B200_API int fdtd_set_face_fractions(AcousticFDTDState* st, const float* vx_frac,
+                                          const float* vy_frac, const float* vz_frac);
+
+/* acoustic_fdtd.h:255-260. */
+FDTD_B200_API int fdtd_sample_plate_weighted(const AcousticFDTDState* st, int n_plate,
+                                             const int* plate_indices, const float* weights,
+                                             float* out_w);
+
+/* acoustic_fdtd.h:279-284. */
+FDTD_B200_API int fdtd_precompute_pressure_samplers(const AcousticFDTDState* st, int n_rec,
+                                                    const float* rec_xyz, int* out_idx8,
+                                                    float* out_wgt8);
+
+/* acoustic_fdtd.h:294-300. */
+FDTD_B200_API int fdtd_precompute_velocity_samplers(const AcousticFDTDState* st, int n_rec,
+                                                    const float* rec_xyz,
+                                                    int* out_vx_idx8, float* out_vx_wgt8,
+                                                    int* out_vy_idx8, float* out_vy_wgt8,
+                                                    int* out_vz_idx8, float* out_vz_wgt8);
+
+/* acoustic_fdtd.h:306-311. */
+FDTD_B200_API int fdtd_sample_pressure_precomputed(const AcousticFDTDState* st, int n_rec,
+                                                   const int* idx8, const float* wgt8,
+                                                   float* out_p);
+
+/* acoustic_fdtd.h:317-324. */
+FDTD_B200_API int fdtd_sample_velocity_precomputed(const AcousticFDTDState* st, int n_rec,
+                                                   const int* vx_idx8, const float* vx_wgt8,
+                                                   const int* vy_idx8, const float* vy_wgt8,
+                                                   const int* vz_idx8, const float* vz_wgt8,
+                                                   float* out_vx, float* out_vy, float* out_vz);
+
+/* acoustic_fdtd.h:338.  Plate update, velocity update, face BCs, pressure
+ * update, and the 256-step stability check, n_steps times. */
+FDTD_B200_API int fdtd_step(AcousticFDTDState* st, int n_steps);
+
+/* acoustic_fdtd.h:341, :344. */
+FDTD_B200_API int fdtd_get_step_count(const AcousticFDTDState* st);
+FDTD_B200_API float fdtd_get_dt(const AcousticFDTDState* st);
+
+/* acoustic_fdtd.h:347.  Zeroes P, V and the plate; keeps geometry. */
+FDTD_B200_API int fdtd_reset(AcousticFDTDState* st);
+
+/* acoustic_fdtd.h:359-363, :372-376. */
+FDTD_B200_API int fdtd_get_pressure_field(const AcousticFDTDState* st, float* out, int out_len);
+FDTD_B200_API int fdtd_get_plate_displacement(const AcousticFDTDState* st, float* out,
+                                              int out_len);
+
+/* acoustic_fdtd.h:396-402. */
+FDTD_B200_API int fdtd_sample_plate_displacement_batch(const AcousticFDTDState* st,
+                                                       int n_points, const int* saddle_idx4,
+                                                       const float* saddle_wgt4, float* out_w);
+
+/* acoustic_fdtd.h:413-418. */
+FDTD_B200_API int fdtd_sample_pressure(const AcousticFDTDState* st, int n_rec,
+                                       const float* rec_xyz, float* out_p);
+
+/* acoustic_fdtd.h:441-446, :449-458. */
+FDTD_B200_API void fdtd_get_velocity_dims(const AcousticFDTDState* st, int* Nvx, int* Nvy,
+                                          int* Nvz);
+FDTD_B200_API int fdtd_get_velocity_x(const AcousticFDTDState* st, float* out, int out_len);
+FDTD_B200_API int fdtd_get_velocity_y(const AcousticFDTDState* st, float* out, int out_len);
+FDTD_B200_API int fdtd_get_velocity_z(const AcousticFDTDState* st, float* out, int out_len);
+
+/* acoustic_fdtd.h:476-483. */
+FDTD_B200_API int fdtd_sample_velocity(const AcousticFDTDState* st, int n_rec,
+                                       const float* rec_xyz, float* out_vx, float* out_vy,
+                                       float* out_vz);
+
+/* acoustic_fdtd.h:499-506. */
+FDTD_B200_API int fdtd_get_surface_emission(const AcousticFDTDState* st, int n_surf,
+                                            const float* surf_xyz, const float* surf_normals,
+                                            float* out_P, float* out_vn);
+
+/* ============================ engine extensions ============================ */
+
+/* Device-memory layout of one field: row stride (floats) and bytes per field. */
+FDTD_B200_API int fdtd_b200_field_layout(int Nx, int Ny, int Nz, int* row_stride,
+                                         size_t* field_bytes);
+
+/* fdtd_create on CUDA device `device` (-1 = current).  When `fields` is
+ * non-NULL it holds eight device pointers {P0, P1, Vx0, Vy0, Vz0, Vx1, Vy1,
+ * Vz1} (two pressure buffers and two velocity sets), each at least
+ * field_bytes long and 16-byte aligned (e.g. torch tensors); the engine uses
+ * them instead of allocating, zeroes them, and never frees them. */
+FDTD_B200_API AcousticFDTDState* fdtd_b200_create_ex(
+    int Nx, int Ny, int Nz, float dx, float c, float rho_air,
+    const uint8_t* cell_type, int plate_iz, const uint8_t* plate_active,
+    float plate_mass_density, float plate_stiffness_D,
+    float plate_alpha_M, float plate_beta_K, int n_pml,
+    int device, float* const* fields);
+
+/* Per-face absorption: a6 = {x_lo, x_hi, y_lo, y_hi, z_lo, z_hi}, each > 0,
+ * scales the PML's sigma_max on that face.  All ones = the reference. */
+FDTD_B200_API int fdtd_b200_set_face_absorption(AcousticFDTDState* st, const float* a6);
+
+/* One pressure deposit with the reference's open-cell rule
+ * (acoustic_fdtd.cpp:840-872); returns the number of cells written. */
+FDTD_B200_API int fdtd_b200_add_pressure(AcousticFDTDState* st, int cell_index, float amp);
+
+/* Point source: before the step that starts at step count n (0 <= n < n_signal)
+ * signal[n] is deposited at cell_index with the open-cell rule.  n_signal = 0
+ * removes the source. */
+FDTD_B200_API int fdtd_b200_set_point_source(AcousticFDTDState* st, int cell_index,
+                                             const float* signal, int n_signal);
+
+/* Receivers: after every step each receiver's 8-tap pressure sample (the
+ * layout of fdtd_precompute_pressure_samplers) is appended to a device trace
+ * of up to `capacity` steps.  n_rec = 0 removes them. */
+FDTD_B200_API int fdtd_b200_set_receivers(AcousticFDTDState* st, int n_rec, const int* idx8,
+                                          const float* wgt8, int capacity);
+
+/* Copies the recorded traces, [n_recorded][n_rec] float32, and clears them. */
+FDTD_B200_API int fdtd_b200_get_traces(AcousticFDTDState* st, float* out, int out_len,
+                                       int* n_recorded);
+
+/* Stream the handle works on (a cudaStream_t; NULL = the handle's own stream). */
+FDTD_B200_API int fdtd_b200_set_stream(AcousticFDTDState* st, void* stream);
+FDTD_B200_API void* fdtd_b200_get_stream(const AcousticFDTDState* st);
+
+/* Launches n_steps without waiting and without stopping at a failed stability
+ * check; the first failure is latched and reported by fdtd_b200_synchronize. */
+FDTD_B200_API int fdtd_b200_step_async(AcousticFDTDState* st, int n_steps);
+
+/* Waits for the handle's stream; returns FDTD_OK, FDTD_ERR_UNSTABLE (latched
+ * by an async step) or FDTD_ERR_CUDA.  Clears the latch. */
+FDTD_B200_API int fdtd_b200_synchronize(AcousticFDTDState* st);
+
+/* Step-kernel selection: 0 automatic (fused single pass for open rooms,
+ * two-pass otherwise), 1 two-pass, 2 fused (rejected with FDTD_ERR_ARG when
+ * the scene has walls, fractions or an active plate). */
+FDTD_B200_API int fdtd_b200_set_kernel(AcousticFDTDState* st, int mode);
+FDTD_B200_API int fdtd_b200_get_kernel(const AcousticFDTDState* st);
+
+/* Device pointers of the current fields: out5 = {P (current), P (next), Vx, Vy, Vz}. */
+FDTD_B200_API int fdtd_b200_device_fields(const AcousticFDTDState* st, void** out5);
+
+/* CUDA-event timing of the main step kernel(s) on the handle's stream. */
+FDTD_B200_API int fdtd_b200_profile(AcousticFDTDState* st, int enable);
+FDTD_B200_API int fdtd_b200_profile_read(AcousticFDTDState* st, double* total_ms,
+                                         long long* launches, long long* kernel_launches);
+
+/* Number of kernels this handle has launched since creation. */
+FDTD_B200_API long long fdtd_b200_launch_count(const AcousticFDTDState* st);
+
+/* Text of the last CUDA error seen by any handle in this process. */
+FDTD_B200_API const char* fdtd_b200_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
