@@ -58,16 +58,28 @@ def parse_args():
                     help="bound on the CPU-baseline sample")
     ap.add_argument("--ref-seconds", type=float, default=90.0,
                     help="bound on the timed part of --impl reference")
-    return ap.parse_args()
+    ap.add_argument("--grid", default=None,
+                    help="NX,NY,NZ: a smaller seeded room of the same kind (profiling only)")
+    args = ap.parse_args()
+    global GRID
+    GRID = tuple(int(v) for v in args.grid.split(",")) if args.grid else None
+    return args
+
+
+GRID = None
 
 
 def workload():
-    from spectral_analyzer_b200.rooms import large_room
+    from spectral_analyzer_b200.rooms import large_room, seeded_room
+    if GRID:
+        r = seeded_room(*GRID, 10000, seed=2, n_rec=8, source_kind="ricker")
+        r.name = "room{}x{}x{}_ricker".format(*GRID)
+        return r
     return large_room(n_steps=10000)
 
 
 def config_dict(room, n, kernel):
-    return {"workload": "room512x384x256_ricker_8rec", "grid": [room.nx, room.ny, room.nz],
+    return {"workload": room.name + "_8rec", "grid": [room.nx, room.ny, room.nz],
             "cells": room.cells, "receivers": len(room.receivers), "source": "ricker_1kHz",
             "absorption": [round(a, 6) for a in room.absorption], "n_pml": room.n_pml,
             "dt_s": room.dt, "courant": 0.77 / 3 ** 0.5, "step_kernel": kernel,
