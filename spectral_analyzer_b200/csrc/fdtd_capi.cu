@@ -136,6 +136,7 @@ struct AcousticFDTDState {
     int stab_phase = 0;
 
     int kernel_mode = 0;
+    FusedCache* fcache = nullptr;    // TMA descriptors of the fields (fused step)
 
     long long launches = 0;          // kernels launched by this handle
 
@@ -449,6 +450,17 @@ int prof_end(AcousticFDTDState* st, cudaEvent_t e1, int kernels)
     return FDTD_OK;
 }
 
+// A fused-step CTA whose bounded load wait ran out leaves its blocks' results
+// incomplete: reported as a CUDA-level failure (status read from h_status).
+int check_timeout(AcousticFDTDState* st)
+{
+    if (st->h_status[kStatusTimeout] == 0xFFFFFFFFu) return FDTD_OK;
+    std::lock_guard<std::mutex> lk(g_err_mu);
+    snprintf(g_err, sizeof(g_err), "fused step: a tile's load wait timed out (block %u)",
+             st->h_status[kStatusTimeout]);
+    return FDTD_ERR_CUDA;
+}
+
 void report_unstable_cell(AcousticFDTDState* st, unsigned q)
 {
     const int ny = st->Ny, nz = st->Nz;
@@ -541,10 +553,12 @@ int one_step(AcousticFDTDState* st, bool sync_check)
             int rc2 = alloc_second_velocity_set(st);
             if (rc2) return rc2;
         }
+        if (!st->fcache) st->fcache = fused_cache_create();
         FusedArgs a{st->g, st->cf, st->tb, st->P(), st->Pn(),
                     {st->V(0), st->V(1), st->V(2)},
-                    {st->v[st->cv ^ 1][0], st->v[st->cv ^ 1][1], st->v[st->cv ^ 1][2]}};
-        CK(launch_fused_step(a, s));
+                    {st->v[st->cv ^ 1][0], st->v[st->cv ^ 1][1], st->v[st->cv ^ 1][2]},
+                    st->d_status};
+        CK(launch_fused_step(a, st->fcache, s));
         ++st->launches;
         st->cv ^= 1;
         if ((rc = prof_end(st, e1, fused_kernel_launches_per_step()))) return rc;
@@ -581,9 +595,10 @@ int one_step(AcousticFDTDState* st, bool sync_check)
         CK(launch_check(st->g, st->P(), st->N, phase, st->d_status, st->step_count, s));
         ++st->launches;
         if (sync_check) {
-            CK(cudaMemcpyAsync(st->h_status + kStatusCell, st->d_status + kStatusCell,
-                               sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(st->h_status, st->d_status, kStatusWords * sizeof(unsigned),
+                               cudaMemcpyDeviceToHost, s));
             CK(cudaStreamSynchronize(s));
+            if (int rc2 = check_timeout(st)) return rc2;
             unsigned bad = st->h_status[kStatusCell];
             if (bad != 0xFFFFFFFFu) {
                 report_unstable_cell(st, bad);
@@ -619,6 +634,7 @@ void free_state(AcousticFDTDState* st)
     cudaFree(st->d_sidx); cudaFree(st->d_sw); cudaFree(st->d_sout);
     cudaFreeHost(st->h_sidx); cudaFreeHost(st->h_sw); cudaFreeHost(st->h_sout);
     for (cudaEvent_t e : st->prof.ev) cudaEventDestroy(e);
+    fused_cache_destroy(st->fcache);
     if (st->own_stream) cudaStreamDestroy(st->own_stream);
     if (d >= 0 && d != st->device) cudaSetDevice(d);
     delete st;
@@ -1247,6 +1263,7 @@ int fdtd_b200_synchronize(AcousticFDTDState* st)
     CK(cudaMemcpyAsync(st->h_status, st->d_status, kStatusWords * sizeof(unsigned),
                        cudaMemcpyDeviceToHost, st->stream));
     CK(cudaStreamSynchronize(st->stream));
+    if (int rc = check_timeout(st)) return rc;
     if (st->h_status[kStatusLatch] != 0xFFFFFFFFu) {
         fprintf(stderr, "[fdtd_pressure] UNSTABLE at step=%u (async)\n", st->h_status[kStatusLatch]);
         CK(cudaMemsetAsync(st->d_status, 0xFF, kStatusWords * sizeof(unsigned), st->stream));

@@ -12,20 +12,25 @@
  *   - computes the new Vx on face f = u-2 of the own columns from P^n planes
  *     f-1 .. f+2 and keeps the last four faces in a register queue;
  *   - computes, for plane i = u-3, the new Vy of rows j0-2 .. j0+TJ and the new
- *     Vz of faces k0-2 .. k0+128: the faces outside the tile are recomputed
- *     here from V^{n-1/2}, never read back from a neighbour, so the step writes
- *     the other velocity set;
+ *     Vz of faces k0-2 .. k0+128: faces outside the tile are recomputed here
+ *     from V^{n-1/2}, never read back from a neighbour, so the step writes the
+ *     other velocity set;
  *   - finishes P^{n+1} of plane i from the 4th-order divergence.
- * Loads go through a ring of shared-memory stages filled with cp.async
- * (16-byte chunks, zero-filled outside the grid) D planes ahead of use; each
- * thread's chunk offsets are computed once, before the march.  Halo rows and
- * columns are shared with neighbouring CTAs that march at the same pace, so
- * they are served mostly from L2.
  *
- * Absorption: inside the x-interior (alpha_x = 0 on the planes involved, all
- * but the 2*n_pml PML planes) a face's damping depends on (j, k) only and is a
- * per-thread constant computed once; PML planes take the general path.  Both
- * paths evaluate the same expression, so results do not depend on the path.
+ * Loads: one thread per CTA issues four TMA boxes per plane (P with a 3-cell
+ * halo in j and a 4-cell halo in k, Vx, Vy with its halo rows, Vz with its halo
+ * columns) into a ring of shared-memory stages D planes ahead of use, each
+ * stage completed by an mbarrier; boxes that reach outside the grid are
+ * zero-filled by the TMA unit.  The box origin in k is k0-4 or k0, a multiple
+ * of 4 floats (16 bytes).  Every mbarrier wait is bounded: a wait that runs
+ * out sets a status word, the CTA drains its copies in flight (again bounded)
+ * and returns.  Halo rows and columns are shared with neighbouring CTAs that
+ * march at the same pace, so they are served mostly from L2.
+ *
+ * Absorption: on x-interior planes (alpha_x = 0, all but the 2*n_pml PML
+ * planes) a face's damping depends on (j, k) only and is a per-thread constant
+ * computed once; PML planes take an out-of-line general path.  Both evaluate
+ * the same expression, so results do not depend on the path.
  *
  * Arithmetic is the reference's (csrc/kernels/acoustic_fdtd.cpp:1099-1148 for
  * the velocity, :894-952 and :1176-1234 for the pressure) with every operation
@@ -33,6 +38,12 @@
  * and to the reference.
  */
 #include "fdtd_internal.h"
+
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
+#include <vector>
 
 namespace fdtd {
 
@@ -44,52 +55,88 @@ struct Cfg {
     static constexpr int TK = 128;              // 32 lanes x float4
     static constexpr int D = D_;                // prefetch distance (iterations)
     static constexpr int NT = 32 * TJ;
-    static constexpr int PR = TJ + 6;           // P stage rows j0-3 .. j0+TJ+2
-    static constexpr int PC = TK + 8;           // P stage cols k0-4 .. k0+TK+3
-    static constexpr int PCH = PC / 4;          // 16-byte chunks per P row (34)
+    static constexpr int PR = TJ + 6;           // P box rows j0-3 .. j0+TJ+2
+    static constexpr int PC = TK + 8;           // P box cols k0-4 .. k0+TK+3
     static constexpr int RING = D + 4;          // planes u-3 .. u in use + D in flight
     static constexpr int VYR = TJ + 3;          // Vy rows j0-2 .. j0+TJ
-    static constexpr int P_STAGE = PR * PC;
-    static constexpr int VX_STAGE = TJ * TK;
-    static constexpr int VY_STAGE = VYR * TK;
-    static constexpr int VZ_STAGE = TJ * PC;    // Vz cols k0-4 .. k0+TK+3
-    static constexpr int V_STAGE = VX_STAGE + VY_STAGE + VZ_STAGE;
+    // box sizes in floats, and stage strides rounded to 128 bytes
+    static constexpr int P_BOX = PR * PC;
+    static constexpr int VX_BOX = TJ * TK;
+    static constexpr int VY_BOX = VYR * TK;
+    static constexpr int VZ_BOX = TJ * PC;      // Vz cols k0-4 .. k0+TK+3
+    static constexpr int r32(int n) { return (n + 31) / 32 * 32; }
+    static constexpr int P_STAGE = r32(P_BOX);
+    static constexpr int VX_OFF = 0;
+    static constexpr int VY_OFF = r32(VX_BOX);
+    static constexpr int VZ_OFF = VY_OFF + r32(VY_BOX);
+    static constexpr int V_STAGE = VZ_OFF + r32(VZ_BOX);
     static constexpr int VSTAGES = D + 1;
     static constexpr int AY_N = TJ + 4;         // alpha_y rows j0-2 .. j0+TJ+1
-    static constexpr int AY_PAD = (AY_N + 3) / 4 * 4;
-    static constexpr int SMEM_FLOATS =
-        RING * P_STAGE + VSTAGES * V_STAGE + VY_STAGE + VZ_STAGE + AY_PAD + PC;
-    static constexpr size_t SMEM_BYTES = sizeof(float) * SMEM_FLOATS;
-    // chunk counts of one iteration's loads and their per-thread share
-    static constexpr int P_CH = PR * PCH;
-    static constexpr int VX_CH = TJ * (TK / 4);
-    static constexpr int VY_CH = VYR * (TK / 4);
-    static constexpr int VZ_CH = TJ * PCH;
-    static constexpr int P_PER = (P_CH + NT - 1) / NT;
-    static constexpr int VY_PER = (VY_CH + NT - 1) / NT;
-    static constexpr int VZ_PER = (VZ_CH + NT - 1) / NT;
-    static_assert(VX_CH == NT, "one Vx chunk per thread");
+    // shared-memory map (floats from a 128-byte aligned base)
+    static constexpr int RING0 = 0;
+    static constexpr int VST0 = RING0 + RING * P_STAGE;
+    static constexpr int VYN0 = VST0 + VSTAGES * V_STAGE;
+    static constexpr int VZN0 = VYN0 + r32(VY_BOX);
+    static constexpr int AY0 = VZN0 + r32(VZ_BOX);
+    static constexpr int AZ0 = AY0 + r32(AY_N);
+    static constexpr int BAR0 = AZ0 + r32(PC);  // RING + VSTAGES mbarriers (8 B each)
+    static constexpr int SMEM_FLOATS = BAR0 + 2 * (RING + VSTAGES);
+    static constexpr size_t SMEM_BYTES = sizeof(float) * SMEM_FLOATS + 128;   // + base alignment
+    static constexpr unsigned P_BYTES = 4u * P_BOX;
+    static constexpr unsigned VX_BYTES = 4u * VX_BOX;
+    static constexpr unsigned VYZ_BYTES = 4u * (VY_BOX + VZ_BOX);
+    static_assert((PC * 4) % 16 == 0 && (TK * 4) % 16 == 0, "TMA box rows are 16-byte multiples");
+    static_assert(PC <= 256 && PR <= 256 && VYR <= 256, "TMA box extent");
     static_assert(VYR <= 2 * TJ, "at most two Vy rows per warp");
+    static_assert(3 * TJ <= 32, "one lane per halo Vz face");
 };
 
-__device__ __forceinline__ void cp_async16(float* smem, const float* gmem, bool valid)
+constexpr int kWaitSpins = 1 << 21;   // bound on mbarrier polls (each poll may block briefly)
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
 {
-    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-    const int n = valid ? 16 : 0;   // 0: the 16 bytes are zero-filled, nothing is read
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(n)
-                 : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
 }
 
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
 
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity)
+{
+    unsigned ok;
+    asm volatile(
+        "{\n .reg .pred p;\n"
+        " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    return ok != 0;
+}
+
+// Bounded wait for the phase with the given parity; false when the bound ran out.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
+{
+    for (int it = 0; it < kWaitSpins; ++it)
+        if (mbar_try(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void tma_load3(unsigned dst, const CUtensorMap* map, int x, int y, int z,
+                                          unsigned bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];\n"
+        ::"r"(dst), "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar) : "memory");
+}
 
 __device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void sts4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 __device__ __forceinline__ void stg4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 __device__ __forceinline__ float& at(float4& v, int q) { return reinterpret_cast<float*>(&v)[q]; }
-__device__ __forceinline__ float at(const float4& v, int q) { return reinterpret_cast<const float*>(&v)[q]; }
 
 // staggered gradient: 4th order in the interior of the face range, else 2nd
 __device__ __forceinline__ float grad4(const Coef& cf, float pm, float p0, float p1, float p2, bool fourth)
@@ -103,16 +150,70 @@ __device__ __forceinline__ float vupd(const Coef& cf, float vold, float grad, fl
     return fmul(fsub(vold, fmul(cf.vc, grad)), damp);
 }
 
-template <class C>
-__global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a, int seg_len, int tiles_k)
+// four faces, 4th-order gradient, given damping (the x-interior fast path)
+__device__ __forceinline__ float4 vel4(const Coef& cf, const float4& pm, const float4& p0,
+                                      const float4& p1, const float4& p2, const float4& vo,
+                                      const float4& dmp)
 {
-    extern __shared__ __align__(16) float smem[];
-    float* const ring = smem;                                  // RING * P_STAGE
-    float* const vst = ring + C::RING * C::P_STAGE;            // VSTAGES * V_STAGE
-    float* const vyn = vst + C::VSTAGES * C::V_STAGE;          // VY_STAGE
-    float* const vzn = vyn + C::VY_STAGE;                      // VZ_STAGE
-    float* const ay_s = vzn + C::VZ_STAGE;                     // AY_PAD
-    float* const az_s = ay_s + C::AY_PAD;                      // PC
+    float4 r;
+    r.x = vupd(cf, vo.x, grad4(cf, pm.x, p0.x, p1.x, p2.x, true), dmp.x);
+    r.y = vupd(cf, vo.y, grad4(cf, pm.y, p0.y, p1.y, p2.y, true), dmp.y);
+    r.z = vupd(cf, vo.z, grad4(cf, pm.z, p0.z, p1.z, p2.z, true), dmp.z);
+    r.w = vupd(cf, vo.w, grad4(cf, pm.w, p0.w, p1.w, p2.w, true), dmp.w);
+    return r;
+}
+
+// as vel4, with a per-face gradient order (bit q of m4) and existence (bit q of ok)
+__device__ __forceinline__ float4 vel4_masked(const Coef& cf, float4 pm, float4 p0, float4 p1,
+                                             float4 p2, float4 vo, float4 dmp, int m4, int ok)
+{
+    float4 r;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float gr = grad4(cf, at(pm, q), at(p0, q), at(p1, q), at(p2, q), (m4 >> q) & 1);
+        at(r, q) = ((ok >> q) & 1) ? vupd(cf, at(vo, q), gr, at(dmp, q)) : 0.0f;
+    }
+    return r;
+}
+
+// General-path velocity of four faces: damping from the alphas.  Out of line
+// so the fast path stays lean (PML planes and ragged tiles only).
+__device__ __noinline__ float4 vel4_general(Coef cf, float4 pm, float4 p0, float4 p1, float4 p2,
+                                            float4 vo, float4 aL, float4 aR, int m4, int ok)
+{
+    float4 dmp;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) at(dmp, q) = face_damp(at(aL, q), at(aR, q), cf.dt);
+    return vel4_masked(cf, pm, p0, p1, p2, vo, dmp, m4, ok);
+}
+
+// P^{n+1} = (P^n - bulk*div) * pd, div = c1*(dx+dy+dz) + c2*(dxx+dyy+dzz)
+__device__ __forceinline__ float pupd(const Coef& cf, float p, float xp, float xm, float xpp,
+                                      float xmm, float yp, float ym, float ypp, float ymm, float zp,
+                                      float zm, float zpp, float zmm, float pd)
+{
+    const float d1 = fadd(fadd(fsub(xp, xm), fsub(yp, ym)), fsub(zp, zm));
+    const float d2 = fadd(fadd(fsub(xpp, xmm), fsub(ypp, ymm)), fsub(zpp, zmm));
+    const float dv = fadd(fmul(cf.c1, d1), fmul(cf.c2, d2));
+    return fmul(fsub(p, fmul(cf.bulk, dv)), pd);
+}
+
+template <class C>
+__global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
+                                                      const __grid_constant__ CUtensorMap tmP,
+                                                      const __grid_constant__ CUtensorMap tmX,
+                                                      const __grid_constant__ CUtensorMap tmY,
+                                                      const __grid_constant__ CUtensorMap tmZ,
+                                                      int seg_len, int tiles_k)
+{
+    extern __shared__ float smem_raw[];
+    float* const smem = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    float* const vyn = smem + C::VYN0;
+    float* const vzn = smem + C::VZN0;
+    float* const ay_s = smem + C::AY0;
+    float* const az_s = smem + C::AZ0;
+    const unsigned sbase = smem_u32(smem);
+    const unsigned bar0 = sbase + 4u * C::BAR0;   // P slot s: bar0 + 8s; V stage v: bar0 + 8(RING+v)
 
     const Grid g = a.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz, sz = g.sz;
@@ -125,101 +226,70 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a, int seg_len, 
     const int i_end = min(i_beg + seg_len, nx);
     const Coef cf = a.cf;
 
-    for (int e = tid; e < C::AY_PAD; e += C::NT) {
+    for (int e = tid; e < C::AY_N; e += C::NT) {
         const int j = j0 - 2 + e;
-        ay_s[e] = (e < C::AY_N && j >= 0 && j < ny) ? __ldg(a.tb.ay + j) : 0.0f;
+        ay_s[e] = (j >= 0 && j < ny) ? __ldg(a.tb.ay + j) : 0.0f;
     }
     for (int e = tid; e < C::PC; e += C::NT) {
         const int k = k0 - 4 + e;
         az_s[e] = (k >= 0 && k < nz) ? __ldg(a.tb.az + k) : 0.0f;
     }
+    if (tid == 0) {
+        for (int q = 0; q < C::RING + C::VSTAGES; ++q) mbar_init(bar0 + 8u * q, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
 
-    // ---- per-thread load descriptors: in-plane element offset of each chunk, -1 = zero fill
-    int p_off[C::P_PER], vy_off[C::VY_PER], vz_off[C::VZ_PER];
-#pragma unroll
-    for (int m = 0; m < C::P_PER; ++m) {
-        const int e = tid + m * C::NT;
-        const int r = e / C::PCH, c4 = e % C::PCH;
-        const int j = j0 - 3 + r, kc = k0 - 4 + 4 * c4;
-        p_off[m] = (e < C::P_CH && j >= 0 && j < ny && kc >= 0 && kc < sz) ? j * sz + kc : -1;
-    }
-    const int vx_off = (j0 + w < ny && k0 + 4 * lane < sz) ? (j0 + w) * sz + k0 + 4 * lane : -1;
-#pragma unroll
-    for (int m = 0; m < C::VY_PER; ++m) {
-        const int e = tid + m * C::NT;
-        const int r = e >> 5, c4 = e & 31;
-        const int j = j0 - 2 + r, kc = k0 + 4 * c4;
-        vy_off[m] = (e < C::VY_CH && j >= 0 && j <= ny - 2 && kc < sz) ? j * sz + kc : -1;
-    }
-#pragma unroll
-    for (int m = 0; m < C::VZ_PER; ++m) {
-        const int e = tid + m * C::NT;
-        const int r = e / C::PCH, c4 = e % C::PCH;
-        const int j = j0 + r, kc = k0 - 4 + 4 * c4;
-        vz_off[m] = (e < C::VZ_CH && j < ny && kc >= 0 && kc < sz) ? j * sz + kc : -1;
-    }
-
-    // Loads feeding iteration u: P plane u, Vx face u-2, Vy/Vz of plane u-3.
-    auto issue = [&](int u, float* pst, float* vs) {
-        const bool pv = (u >= 0 && u < nx);
-        const float* pb = a.p + (pv ? u : 0) * PL;
-#pragma unroll
-        for (int m = 0; m < C::P_PER; ++m) {
-            const int e = tid + m * C::NT;
-            if (e < C::P_CH) {
-                const bool v = pv && p_off[m] >= 0;
-                cp_async16(pst + 4 * e, v ? pb + p_off[m] : a.p, v);
-            }
+    // Loads feeding iteration u (issued by thread 0): P plane u, Vx face u-2,
+    // Vy/Vz of plane u-3.  An iteration without V loads still completes its V
+    // stage's phase (expect_tx of 0 bytes is a plain arrive).
+    auto issue = [&](int u, int ps, int vsg) {
+        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+        const unsigned pb = bar0 + 8u * ps;
+        mbar_expect_tx(pb, C::P_BYTES);
+        tma_load3(sbase + 4u * (C::RING0 + ps * C::P_STAGE), &tmP, k0 - 4, j0 - 3, u, pb);
+        const int f = u - 2, io = u - 3;
+        const bool vx = (u >= i_beg && f >= 0 && f <= nx - 2);
+        const bool vyz = (io >= i_beg && io < i_end);
+        const unsigned vb = bar0 + 8u * (C::RING + vsg);
+        const unsigned vdst = sbase + 4u * (C::VST0 + vsg * C::V_STAGE);
+        mbar_expect_tx(vb, (vx ? C::VX_BYTES : 0u) + (vyz ? C::VYZ_BYTES : 0u));
+        if (vx) tma_load3(vdst + 4u * C::VX_OFF, &tmX, k0, j0, f, vb);
+        if (vyz) {
+            tma_load3(vdst + 4u * C::VY_OFF, &tmY, k0, j0 - 2, io, vb);
+            tma_load3(vdst + 4u * C::VZ_OFF, &tmZ, k0 - 4, j0, io, vb);
         }
-        const int f = u - 2;
-        if (u >= i_beg && f >= 0 && f <= nx - 2) {
-            const bool v = vx_off >= 0;
-            cp_async16(vs + 4 * tid, v ? a.vin[0] + f * PL + vx_off : a.vin[0], v);
-        }
-        const int io = u - 3;
-        if (io >= i_beg && io < i_end) {
-            const float* yb = a.vin[1] + io * PL;
-            const float* zb = a.vin[2] + io * PL;
-#pragma unroll
-            for (int m = 0; m < C::VY_PER; ++m) {
-                const int e = tid + m * C::NT;
-                if (e < C::VY_CH) {
-                    const bool v = vy_off[m] >= 0;
-                    cp_async16(vs + C::VX_STAGE + 4 * e, v ? yb + vy_off[m] : a.vin[1], v);
-                }
-            }
-#pragma unroll
-            for (int m = 0; m < C::VZ_PER; ++m) {
-                const int e = tid + m * C::NT;
-                if (e < C::VZ_CH) {
-                    const bool v = vz_off[m] >= 0;
-                    cp_async16(vs + C::VX_STAGE + C::VY_STAGE + 4 * e, v ? zb + vz_off[m] : a.vin[2], v);
-                }
-            }
-        }
-        cp_async_commit();
     };
 
     const int u0 = i_beg - 3, u1 = i_end + 2;
-    // ring slots, rotated by pointer (slot of plane u-3 .. u, then the D in flight)
-    float* pslot[C::RING];
+    // Slot ids, rotated each iteration.  At iteration u: pslot[0..3] hold planes
+    // u-3 .. u, pslot[4 .. 3+D-1] planes u+1 .. u+D-1 in flight, pslot[3+D] is
+    // free; vslot[0] holds iteration u's V data, vslot[1 .. D-1] the next
+    // iterations' in flight, vslot[D] is free.  pph/vph: parity to wait for, per slot.
+    int pslot[C::RING], vslot[C::VSTAGES];
 #pragma unroll
-    for (int q = 0; q < C::RING; ++q) pslot[q] = ring + q * C::P_STAGE;
-    float* vslot[C::VSTAGES];
+    for (int q = 0; q < C::RING; ++q) pslot[q] = q;
 #pragma unroll
-    for (int q = 0; q < C::VSTAGES; ++q) vslot[q] = vst + q * C::V_STAGE;
-    // At iteration u: pslot[0..3] hold planes u-3 .. u, pslot[4 .. 3+D-1] planes
-    // u+1 .. u+D-1 in flight, pslot[3+D] is free; vslot[0] holds iteration u's V
-    // data, vslot[1 .. D-1] the next iterations' in flight, vslot[D] is free.
-#pragma unroll
-    for (int q = 0; q < C::D; ++q) issue(u0 + q, pslot[3 + q], vslot[q]);
-    __syncthreads();   // alpha tables
+    for (int q = 0; q < C::VSTAGES; ++q) vslot[q] = q;
+    unsigned pph = 0, vph = 0;
+    if (tid == 0)
+        for (int q = 0; q < C::D; ++q) issue(u0 + q, pslot[3 + q], vslot[q]);
 
     // ---- per-thread constants of the own row and columns
     const int jr = j0 + w;
     const int kb = k0 + 4 * lane;                 // first own k
     const bool row_ok = jr < ny;
-    const bool st_ok = row_ok && kb < sz;         // float4 store stays inside the row
+    const bool kfull = k0 + C::TK <= nz;          // every own k of the CTA is a cell
+    const bool st_ok = row_ok && kb < sz;         // the float4 store stays inside the row
+    const int own = row_ok ? jr * sz + kb : 0;    // in-plane offset of the own float4
+    const int cP = (w + 3) * C::PC + 4 * lane + 4;    // own cells in a P stage
+    int zm4 = 0, zok = 0;                         // own Vz faces: 4th order / existing
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int kf = kb + q;
+        zm4 |= (kf > 0 && kf < nz - 2) ? (1 << q) : 0;
+        zok |= (kf <= nz - 2) ? (1 << q) : 0;
+    }
     float4 myz, mpz, dxi, dzi;
     {
         const float pyj = row_ok ? __ldg(a.tb.py + jr) : 1.0f;
@@ -234,12 +304,13 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a, int seg_len, 
             at(dzi, q) = face_damp(fmaxf(ayj, azk), fmaxf(ayj, az_s[4 * lane + 5 + q]), cf.dt);
         }
     }
-    // Vy items of this thread: row w (all warps) and row TJ+w (warps 0..2)
+    // Vy items of this thread: row w (all warps) and row TJ+w (the first VYR-TJ warps)
     constexpr int NY_IT = 2;
     float4 dyi[NY_IT];
 #pragma unroll
     for (int m = 0; m < NY_IT; ++m) {
         const int r = m == 0 ? w : C::TJ + w;
+        dyi[m] = make_float4(1.f, 1.f, 1.f, 1.f);
         if (r < C::VYR) {
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
@@ -249,11 +320,23 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a, int seg_len, 
         }
     }
     float4 qx0 = make_float4(0.f, 0.f, 0.f, 0.f), qx1 = qx0, qx2 = qx0, qx3 = qx0;
+    int u_fail = u1 + 1;   // iteration whose wait ran out (none)
 
     for (int u = u0; u <= u1; ++u) {
-        cp_async_wait<C::D - 1>();
-        __syncthreads();
-        const float* vs = vslot[0];
+        // wait for plane u (P) and iteration u's V data; the decision to stop on a
+        // timeout is made by the whole CTA (the barrier below is also the one that
+        // separates the previous iteration's reads from this iteration's writes)
+        const int ps = pslot[3], vsg = vslot[0];
+        const bool ok = mbar_wait(bar0 + 8u * ps, (pph >> ps) & 1u) &&
+                        mbar_wait(bar0 + 8u * (C::RING + vsg), (vph >> vsg) & 1u);
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicMin(a.status + kStatusTimeout, blockIdx.x + gridDim.x * blockIdx.y);
+            u_fail = u;
+            break;
+        }
+        pph ^= 1u << ps;
+        vph ^= 1u << vsg;
+        const float* vs = smem + C::VST0 + vsg * C::V_STAGE;
 
         // ---- new Vx on face f = u-2 of the own columns (planes f-1 .. f+2) ----
         if (u >= i_beg) {
@@ -262,143 +345,148 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a, int seg_len, 
             if (f >= 0 && f <= nx - 2 && row_ok) {
                 const bool fourth = (f > 0 && f < nx - 2);
                 const float axf = __ldg(a.tb.ax + f), axf1 = __ldg(a.tb.ax + f + 1);
-                const bool xint = (axf == 0.0f && axf1 == 0.0f);
-                const int co = (w + 3) * C::PC + 4 * lane + 4;
-                const float4 pm = lds4(pslot[0] + co), p0 = lds4(pslot[1] + co);
-                const float4 p1 = lds4(pslot[2] + co), p2 = lds4(pslot[3] + co);
-                const float4 vo = lds4(vs + 4 * tid);
+                const float4 pm = lds4(smem + C::RING0 + pslot[0] * C::P_STAGE + cP);
+                const float4 p0 = lds4(smem + C::RING0 + pslot[1] * C::P_STAGE + cP);
+                const float4 p1 = lds4(smem + C::RING0 + pslot[2] * C::P_STAGE + cP);
+                const float4 p2 = lds4(smem + C::RING0 + pslot[3] * C::P_STAGE + cP);
+                const float4 vo = lds4(vs + C::VX_OFF + 4 * tid);
+                if (fourth && axf == 0.0f && axf1 == 0.0f && kfull) {
+                    vnew = vel4(cf, pm, p0, p1, p2, vo, dxi);
+                } else {
+                    float4 aL, aR;
+                    int okx = 0;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const float gr = grad4(cf, at(pm, q), at(p0, q), at(p1, q), at(p2, q), fourth);
-                    const float dmp = xint ? at(dxi, q)
-                        : face_damp(fmaxf(axf, at(myz, q)), fmaxf(axf1, at(myz, q)), cf.dt);
-                    at(vnew, q) = (kb + q < nz) ? vupd(cf, at(vo, q), gr, dmp) : 0.0f;
+                    for (int q = 0; q < 4; ++q) {
+                        at(aL, q) = fmaxf(axf, at(myz, q));
+                        at(aR, q) = fmaxf(axf1, at(myz, q));
+                        okx |= (kb + q < nz) ? (1 << q) : 0;
+                    }
+                    vnew = vel4_general(cf, pm, p0, p1, p2, vo, aL, aR, fourth ? 15 : 0, okx);
                 }
-                if (f >= i_beg && f < i_end && st_ok) stg4(a.vout[0] + f * PL + (long long)jr * sz + kb, vnew);
+                if (f >= i_beg && f < i_end && st_ok) stg4(a.vout[0] + f * PL + own, vnew);
             }
             qx0 = qx1; qx1 = qx2; qx2 = qx3; qx3 = vnew;
         }
 
         // ---- plane i = u-3: new Vy / Vz (with halos), then P^{n+1} ----
-        const int i = u - 3;
-        if (i >= i_beg) {
-            const float axi = __ldg(a.tb.ax + i);
-            const bool xint = (axi == 0.0f);
-            const float* pst = pslot[0];
-            const float* vys = vs + C::VX_STAGE;
-            const float* vzs = vys + C::VY_STAGE;
-            const long long ib = i * PL;
+        {
+            const int i = u - 3;
+            if (i >= i_beg) {
+                const float axi = __ldg(a.tb.ax + i);
+                const bool xint = (axi == 0.0f);
+                const float* pst = smem + C::RING0 + pslot[0] * C::P_STAGE;
+                const float* vys = vs + C::VY_OFF;
+                const float* vzs = vs + C::VZ_OFF;
+                const long long ib = i * PL;
 
-            // Vy rows: row w, and row TJ+w for the first three warps
+                // Vy rows: row w, and row TJ+w for the first VYR-TJ warps
 #pragma unroll
-            for (int m = 0; m < NY_IT; ++m) {
-                const int r = m == 0 ? w : C::TJ + w;
-                if (r < C::VYR) {
-                    const int jf = j0 - 2 + r;
+                for (int m = 0; m < NY_IT; ++m) {
+                    const int r = m == 0 ? w : C::TJ + w;
+                    if (r < C::VYR) {
+                        const int jf = j0 - 2 + r;
+                        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (jf >= 0 && jf <= ny - 2) {
+                            const bool fourth = (jf > 0 && jf < ny - 2);
+                            const float* pc = pst + 4 * lane + 4;
+                            const float4 pm = lds4(pc + r * C::PC), p0 = lds4(pc + (r + 1) * C::PC);
+                            const float4 p1 = lds4(pc + (r + 2) * C::PC), p2 = lds4(pc + (r + 3) * C::PC);
+                            const float4 vo = lds4(vys + r * C::TK + 4 * lane);
+                            if (fourth && xint && kfull) {
+                                v = vel4(cf, pm, p0, p1, p2, vo, dyi[m]);
+                            } else {
+                                float4 aL, aR;
+                                int oky = 0;
+#pragma unroll
+                                for (int q = 0; q < 4; ++q) {
+                                    const float azk = az_s[4 * lane + 4 + q];
+                                    at(aL, q) = fmaxf(fmaxf(axi, ay_s[r]), azk);
+                                    at(aR, q) = fmaxf(fmaxf(axi, ay_s[r + 1]), azk);
+                                    oky |= (kb + q < nz) ? (1 << q) : 0;
+                                }
+                                v = vel4_general(cf, pm, p0, p1, p2, vo, aL, aR, fourth ? 15 : 0, oky);
+                            }
+                            if (r >= 2 && r < C::TJ + 2 && kb < sz)
+                                stg4(a.vout[1] + ib + (long long)jf * sz + kb, v);
+                        }
+                        sts4(vyn + r * C::TK + 4 * lane, v);
+                    }
+                }
+
+                // Vz: own faces kb .. kb+3 of row jr
+                float4 pown = make_float4(0.f, 0.f, 0.f, 0.f);
+                {
+                    const float* prow = pst + (w + 3) * C::PC;
                     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (jf >= 0 && jf <= ny - 2) {
-                        const bool fourth = (jf > 0 && jf < ny - 2);
-                        const float* pc = pst + 4 * lane + 4;
-                        const float4 pm = lds4(pc + r * C::PC), p0 = lds4(pc + (r + 1) * C::PC);
-                        const float4 p1 = lds4(pc + (r + 2) * C::PC), p2 = lds4(pc + (r + 3) * C::PC);
-                        const float4 vo = lds4(vys + r * C::TK + 4 * lane);
+                    if (row_ok) {
+                        const int c = 4 * lane + 4;            // col of kb
+                        pown = lds4(prow + c);
+                        const float4 pb4 = lds4(prow + c + 4);
+                        const float pl = prow[c - 1];
+                        const float4 vo = lds4(vzs + w * C::PC + c);
+                        // faces kb+q use P[kb+q-1 .. kb+q+2]
+                        const float4 pm = make_float4(pl, pown.x, pown.y, pown.z);
+                        const float4 p1 = make_float4(pown.y, pown.z, pown.w, pb4.x);
+                        const float4 p2 = make_float4(pown.z, pown.w, pb4.x, pb4.y);
+                        if (xint) {
+                            v = vel4_masked(cf, pm, pown, p1, p2, vo, dzi, zm4, zok);
+                        } else {
+                            const float ay = ay_s[w + 2];
+                            float4 aL, aR;
 #pragma unroll
-                        for (int q = 0; q < 4; ++q) {
-                            const float gr = grad4(cf, at(pm, q), at(p0, q), at(p1, q), at(p2, q), fourth);
-                            float dmp;
-                            if (xint) {
-                                dmp = at(dyi[m], q);
-                            } else {
-                                const float azk = az_s[4 * lane + 4 + q];
-                                dmp = face_damp(fmaxf(fmaxf(axi, ay_s[r]), azk),
-                                                fmaxf(fmaxf(axi, ay_s[r + 1]), azk), cf.dt);
+                            for (int q = 0; q < 4; ++q) {
+                                at(aL, q) = fmaxf(fmaxf(axi, ay), az_s[c + q]);
+                                at(aR, q) = fmaxf(fmaxf(axi, ay), az_s[c + q + 1]);
                             }
-                            at(v, q) = (kb + q < nz) ? vupd(cf, at(vo, q), gr, dmp) : 0.0f;
+                            v = vel4_general(cf, pm, pown, p1, p2, vo, aL, aR, zm4, zok);
                         }
-                        if (r >= 2 && r < C::TJ + 2 && kb < sz)
-                            stg4(a.vout[1] + ib + (long long)jf * sz + kb, v);
+                        if (st_ok) stg4(a.vout[2] + ib + own, v);
                     }
-                    sts4(vyn + r * C::TK + 4 * lane, v);
+                    sts4(vzn + w * C::PC + 4 * lane + 4, v);
                 }
-            }
+                // halo Vz faces k0-2, k0-1, k0+TK of every row: 3*TJ faces, one per
+                // lane of the last warp
+                if (w == C::TJ - 1 && lane < 3 * C::TJ) {
+                    const int jl = lane / 3, which = lane - 3 * jl;
+                    const int ch = which < 2 ? 2 + which : C::TK + 4;
+                    const int kf = k0 - 4 + ch;
+                    const float* prow = pst + (jl + 3) * C::PC;
+                    float vh = 0.0f;
+                    if (j0 + jl < ny && kf >= 0 && kf <= nz - 2) {
+                        const bool fourth = (kf > 0 && kf < nz - 2);
+                        const float ay = ay_s[jl + 2];
+                        const float gr = grad4(cf, prow[ch - 1], prow[ch], prow[ch + 1], prow[ch + 2], fourth);
+                        const float dmp = face_damp(fmaxf(fmaxf(axi, ay), az_s[ch]),
+                                                    fmaxf(fmaxf(axi, ay), az_s[ch + 1]), cf.dt);
+                        vh = vupd(cf, vzs[jl * C::PC + ch], gr, dmp);
+                    }
+                    vzn[jl * C::PC + ch] = vh;
+                }
+                __syncthreads();
 
-            // Vz: own faces kb .. kb+3 of row jr, plus halo faces k0-2, k0-1 (lane 0)
-            // and k0+TK (lane 31)
-            {
-                const float* prow = pst + (w + 3) * C::PC;
-                const float* vzr = vzs + w * C::PC;
-                float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+                // P^{n+1} of the own cells
                 if (row_ok) {
-                    const int c = 4 * lane + 4;            // col of kb
-                    const float4 pa = lds4(prow + c), pb = lds4(prow + c + 4);
-                    const float pl = prow[c - 1];
-                    const float4 vo = lds4(vzr + c);
-                    const float pv[7] = {pl, pa.x, pa.y, pa.z, pa.w, pb.x, pb.y};
+                    const float* yr = vyn + 4 * lane;
+                    const float4 ymm = lds4(yr + w * C::TK), ym = lds4(yr + (w + 1) * C::TK);
+                    const float4 yp = lds4(yr + (w + 2) * C::TK), ypp = lds4(yr + (w + 3) * C::TK);
+                    const float* zr = vzn + w * C::PC + 4 * lane;
+                    const float2 za = *reinterpret_cast<const float2*>(zr + 2);   // faces kb-2, kb-1
+                    const float4 zb = lds4(zr + 4);                                // faces kb .. kb+3
+                    const float zc = zr[8];                                        // face kb+4
+                    // px[i] = 1 on x-interior planes, so min(px[i], min(py, pz)) = mpz there
+                    const float pxi = __ldg(a.tb.px + i);
+                    float4 out;
+                    out.x = pupd(cf, pown.x, qx2.x, qx1.x, qx3.x, qx0.x, yp.x, ym.x, ypp.x, ymm.x, zb.x, za.y, zb.y, za.x, fminf(pxi, mpz.x));
+                    out.y = pupd(cf, pown.y, qx2.y, qx1.y, qx3.y, qx0.y, yp.y, ym.y, ypp.y, ymm.y, zb.y, zb.x, zb.z, za.y, fminf(pxi, mpz.y));
+                    out.z = pupd(cf, pown.z, qx2.z, qx1.z, qx3.z, qx0.z, yp.z, ym.z, ypp.z, ymm.z, zb.z, zb.y, zb.w, zb.x, fminf(pxi, mpz.z));
+                    out.w = pupd(cf, pown.w, qx2.w, qx1.w, qx3.w, qx0.w, yp.w, ym.w, ypp.w, ymm.w, zb.w, zb.z, zc, zb.y, fminf(pxi, mpz.w));
+                    if (!kfull) {
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const int kf = kb + q;
-                        if (kf <= nz - 2) {
-                            const bool fourth = (kf > 0 && kf < nz - 2);
-                            const float gr = grad4(cf, pv[q], pv[q + 1], pv[q + 2], pv[q + 3], fourth);
-                            float dmp;
-                            if (xint) {
-                                dmp = at(dzi, q);
-                            } else {
-                                const float ay = ay_s[w + 2];
-                                dmp = face_damp(fmaxf(fmaxf(axi, ay), az_s[c + q]),
-                                                fmaxf(fmaxf(axi, ay), az_s[c + q + 1]), cf.dt);
-                            }
-                            at(v, q) = vupd(cf, at(vo, q), gr, dmp);
-                        }
+                        for (int q = 0; q < 4; ++q)
+                            if (kb + q >= nz) at(out, q) = 0.0f;
                     }
-                    if (st_ok) stg4(a.vout[2] + ib + (long long)jr * sz + kb, v);
-                    // halo faces: lane 0 -> cols 2, 3; lane 31 -> col TK+4
-                    if (lane == 0 || lane == 31) {
-                        const float ay = ay_s[w + 2];
-#pragma unroll
-                        for (int h = 0; h < 2; ++h) {
-                            const int ch = lane == 0 ? 2 + h : C::TK + 4;
-                            if (lane == 31 && h == 1) break;
-                            const int kf = k0 - 4 + ch;
-                            float vh = 0.0f;
-                            if (kf >= 0 && kf <= nz - 2) {
-                                const bool fourth = (kf > 0 && kf < nz - 2);
-                                const float gr = grad4(cf, prow[ch - 1], prow[ch], prow[ch + 1], prow[ch + 2], fourth);
-                                const float dmp = face_damp(fmaxf(fmaxf(axi, ay), az_s[ch]),
-                                                            fmaxf(fmaxf(axi, ay), az_s[ch + 1]), cf.dt);
-                                vh = vupd(cf, vzr[ch], gr, dmp);
-                            }
-                            vzn[w * C::PC + ch] = vh;
-                        }
-                    }
+                    if (kb < sz) stg4(a.pn + ib + own, out);
                 }
-                sts4(vzn + w * C::PC + 4 * lane + 4, v);
-            }
-            __syncthreads();
-
-            // P^{n+1} of the own cells
-            if (row_ok) {
-                const float* yr = vyn + 4 * lane;
-                const float4 ymm = lds4(yr + w * C::TK), ym = lds4(yr + (w + 1) * C::TK);
-                const float4 yp = lds4(yr + (w + 2) * C::TK), ypp = lds4(yr + (w + 3) * C::TK);
-                const float* zr = vzn + w * C::PC + 4 * lane;
-                const float4 za = lds4(zr), zb = lds4(zr + 4), zc = lds4(zr + 8);
-                const float zv[9] = {za.z, za.w, zb.x, zb.y, zb.z, zb.w, zc.x, zc.y, zc.z};
-                const float4 pc = lds4(pst + (w + 3) * C::PC + 4 * lane + 4);
-                const float pxi = xint ? 1.0f : __ldg(a.tb.px + i);
-                float4 out;
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    // zv[q + 2] = face k, +1 = k-1, +3 = k+1, +0 = k-2
-                    const float d1 = fadd(fadd(fsub(at(qx2, q), at(qx1, q)), fsub(at(yp, q), at(ym, q))),
-                                          fsub(zv[q + 2], zv[q + 1]));
-                    const float d2 = fadd(fadd(fsub(at(qx3, q), at(qx0, q)), fsub(at(ypp, q), at(ymm, q))),
-                                          fsub(zv[q + 3], zv[q]));
-                    const float dv = fadd(fmul(cf.c1, d1), fmul(cf.c2, d2));
-                    const float pd = xint ? at(mpz, q) : fminf(pxi, at(mpz, q));
-                    at(out, q) = (kb + q < nz) ? fmul(fsub(at(pc, q), fmul(cf.bulk, dv)), pd) : 0.0f;
-                }
-                if (kb < sz) stg4(a.pn + ib + (long long)jr * sz + kb, out);
             }
         }
 
@@ -406,18 +494,30 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a, int seg_len, 
         // The slots receiving iteration u+D's loads (pslot[3+D-1], vslot[D-1]) were
         // freed one iteration ago: their last reads (plane u-4, iteration u-1)
         // happened before this iteration's first barrier.
-        float* pfree = pslot[0];
+        {
+            const int pfree = pslot[0];
 #pragma unroll
-        for (int q = 0; q + 1 < C::RING; ++q) pslot[q] = pslot[q + 1];
-        pslot[C::RING - 1] = pfree;
-        float* vfree = vslot[0];
+            for (int q = 0; q + 1 < C::RING; ++q) pslot[q] = pslot[q + 1];
+            pslot[C::RING - 1] = pfree;
+            const int vfree = vslot[0];
 #pragma unroll
-        for (int q = 0; q + 1 < C::VSTAGES; ++q) vslot[q] = vslot[q + 1];
-        vslot[C::VSTAGES - 1] = vfree;
-        if (u + C::D <= u1) issue(u + C::D, pslot[3 + C::D - 1], vslot[C::D - 1]);
-        else cp_async_commit();
+            for (int q = 0; q + 1 < C::VSTAGES; ++q) vslot[q] = vslot[q + 1];
+            vslot[C::VSTAGES - 1] = vfree;
+            if (tid == 0 && u + C::D <= u1) issue(u + C::D, pslot[3 + C::D - 1], vslot[C::D - 1]);
+        }
     }
-    cp_async_wait<0>();
+
+    // A normal march waits for every load it issued, so none is in flight here.
+    // After a timed-out wait at iteration u_fail, the copies issued for
+    // iterations u_fail .. u_fail+D-1 may still be landing: wait for them
+    // (bounded) before the CTA's shared memory is released.
+    if (u_fail <= u1 && tid == 0) {
+        for (int q = 0; q < C::D && u_fail + q <= u1; ++q) {
+            const int ps = pslot[3 + q], vsg = vslot[q];
+            mbar_wait(bar0 + 8u * ps, (pph >> ps) & 1u);
+            mbar_wait(bar0 + 8u * (C::RING + vsg), (vph >> vsg) & 1u);
+        }
+    }
 }
 
 using FusedCfg = Cfg<8, 2>;
@@ -427,7 +527,66 @@ int g_slots_per_sm[kMaxDevices];
 int g_sms[kMaxDevices];
 bool g_configured[kMaxDevices];
 
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+std::once_flag g_encode_once;
+
+cudaError_t get_encoder()
+{
+    std::call_once(g_encode_once, [] {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    });
+    return g_encode ? cudaSuccess : cudaErrorNotSupported;
+}
+
+// A 3-D map over one padded field [nx][ny][sz] with a (bx, by, 1) box.
+cudaError_t encode_map(CUtensorMap* m, const float* base, const Grid& g, int bx, int by)
+{
+    cudaError_t e = get_encoder();
+    if (e != cudaSuccess) return e;
+    cuuint64_t dims[3] = {(cuuint64_t)g.sz, (cuuint64_t)g.ny, (cuuint64_t)g.nx};
+    cuuint64_t strides[2] = {(cuuint64_t)g.sz * 4, (cuuint64_t)g.plane * 4};
+    cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
+    cuuint32_t es[3] = {1, 1, 1};
+    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides,
+                          box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
+}
+
 }  // namespace
+
+struct FusedCache {
+    struct Entry {
+        const float* base;
+        int kind;
+        CUtensorMap map;
+    };
+    std::vector<Entry> entries;
+};
+
+FusedCache* fused_cache_create() { return new FusedCache(); }
+void fused_cache_destroy(FusedCache* c) { delete c; }
+
+static cudaError_t cached_map(FusedCache* c, const float* base, int kind, const Grid& g, CUtensorMap* out)
+{
+    for (const auto& e : c->entries)
+        if (e.base == base && e.kind == kind) { *out = e.map; return cudaSuccess; }
+    using C = FusedCfg;
+    static const int bx[4] = {C::PC, C::TK, C::TK, C::PC};
+    static const int by[4] = {C::PR, C::TJ, C::VYR, C::TJ};
+    FusedCache::Entry e;
+    e.base = base;
+    e.kind = kind;
+    cudaError_t err = encode_map(&e.map, base, g, bx[kind], by[kind]);
+    if (err != cudaSuccess) return err;
+    c->entries.push_back(e);
+    *out = e.map;
+    return cudaSuccess;
+}
 
 bool fused_supported(const Grid& g)
 {
@@ -436,7 +595,7 @@ bool fused_supported(const Grid& g)
 
 int fused_kernel_launches_per_step() { return 1; }
 
-cudaError_t launch_fused_step(const FusedArgs& a, cudaStream_t s)
+cudaError_t launch_fused_step(const FusedArgs& a, FusedCache* cache, cudaStream_t s)
 {
     using C = FusedCfg;
     int dev = 0;
@@ -456,6 +615,12 @@ cudaError_t launch_fused_step(const FusedArgs& a, cudaStream_t s)
         g_configured[dev] = true;
     }
     const Grid& g = a.g;
+    CUtensorMap maps[4];
+    const float* bases[4] = {a.p, a.vin[0], a.vin[1], a.vin[2]};
+    for (int q = 0; q < 4; ++q) {
+        e = cached_map(cache, bases[q], q, g, &maps[q]);
+        if (e != cudaSuccess) return e;
+    }
     const int tiles_j = (g.ny + C::TJ - 1) / C::TJ;
     const int tiles_k = (g.nz + C::TK - 1) / C::TK;
     const long long tiles = (long long)tiles_j * tiles_k;
@@ -468,7 +633,8 @@ cudaError_t launch_fused_step(const FusedArgs& a, cudaStream_t s)
     const int seg_len = (int)((g.nx + segs - 1) / segs);
     segs = (g.nx + seg_len - 1) / seg_len;
     dim3 grid((unsigned)tiles, (unsigned)segs, 1);
-    k_fused_step<C><<<grid, C::NT, C::SMEM_BYTES, s>>>(a, seg_len, tiles_k);
+    k_fused_step<C><<<grid, C::NT, C::SMEM_BYTES, s>>>(a, maps[0], maps[1], maps[2], maps[3], seg_len,
+                                                       tiles_k);
     return cudaGetLastError();
 }
 

@@ -65,8 +65,10 @@ struct Deposit {
     long long idx[6];
 };
 
-// Status words (unsigned, 0xFFFFFFFF = none), reset with a 0xFF memset.
-enum StatusSlot { kStatusCell = 0, kStatusPlate = 1, kStatusLatch = 2, kStatusWords = 4 };
+// Status words (unsigned, 0xFFFFFFFF = none), reset with a 0xFF memset:
+// first unstable cell of a check, first unstable plate node, first failing
+// step latched by async stepping, and a fused-step CTA whose load wait ran out.
+enum StatusSlot { kStatusCell = 0, kStatusPlate = 1, kStatusLatch = 2, kStatusTimeout = 3, kStatusWords = 4 };
 
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
 __device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
@@ -110,9 +112,13 @@ struct FusedArgs {
     float* pn;             // P^{n+1}
     const float* vin[3];   // V^{n-1/2}: Vx, Vy, Vz
     float* vout[3];        // V^{n+1/2}
+    unsigned* status;      // kStatusTimeout is set if a load wait runs out
 };
+struct FusedCache;         // host-side TMA descriptors of a handle's fields
+FusedCache* fused_cache_create();
+void fused_cache_destroy(FusedCache* c);
 bool fused_supported(const Grid& g);
-cudaError_t launch_fused_step(const FusedArgs& a, cudaStream_t s);
+cudaError_t launch_fused_step(const FusedArgs& a, FusedCache* cache, cudaStream_t s);
 int fused_kernel_launches_per_step();
 
 }  // namespace fdtd
