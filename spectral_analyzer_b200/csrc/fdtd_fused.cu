@@ -321,6 +321,12 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
     }
     float4 qx0 = make_float4(0.f, 0.f, 0.f, 0.f), qx1 = qx0, qx2 = qx0, qx3 = qx0;
     int u_fail = u1 + 1;   // iteration whose wait ran out (none)
+    // alpha_x / px window: at iteration u, axw{3,2,1,0} = alpha_x[u-3 .. u] and
+    // pxw = px[u-3]; the next iteration's values are prefetched one iteration ahead
+    auto ax_at = [&](int q) { return (q >= 0 && q < nx) ? __ldg(a.tb.ax + q) : 0.0f; };
+    auto px_at = [&](int q) { return (q >= 0 && q < nx) ? __ldg(a.tb.px + q) : 1.0f; };
+    float axw3 = ax_at(u0 - 3), axw2 = ax_at(u0 - 2), axw1 = ax_at(u0 - 1), axw0 = ax_at(u0);
+    float pxw = px_at(u0 - 3);
 
     for (int u = u0; u <= u1; ++u) {
         // wait for plane u (P) and iteration u's V data; the decision to stop on a
@@ -336,6 +342,7 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
         }
         pph ^= 1u << ps;
         vph ^= 1u << vsg;
+        const float ax_next = ax_at(u + 1), px_next = px_at(u - 2);
         const float* vs = smem + C::VST0 + vsg * C::V_STAGE;
 
         // ---- new Vx on face f = u-2 of the own columns (planes f-1 .. f+2) ----
@@ -344,7 +351,7 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
             float4 vnew = make_float4(0.f, 0.f, 0.f, 0.f);
             if (f >= 0 && f <= nx - 2 && row_ok) {
                 const bool fourth = (f > 0 && f < nx - 2);
-                const float axf = __ldg(a.tb.ax + f), axf1 = __ldg(a.tb.ax + f + 1);
+                const float axf = axw2, axf1 = axw1;     // alpha_x[f], alpha_x[f+1]
                 const float4 pm = lds4(smem + C::RING0 + pslot[0] * C::P_STAGE + cP);
                 const float4 p0 = lds4(smem + C::RING0 + pslot[1] * C::P_STAGE + cP);
                 const float4 p1 = lds4(smem + C::RING0 + pslot[2] * C::P_STAGE + cP);
@@ -372,7 +379,7 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
         {
             const int i = u - 3;
             if (i >= i_beg) {
-                const float axi = __ldg(a.tb.ax + i);
+                const float axi = axw3;                  // alpha_x[i]
                 const bool xint = (axi == 0.0f);
                 const float* pst = smem + C::RING0 + pslot[0] * C::P_STAGE;
                 const float* vys = vs + C::VY_OFF;
@@ -474,7 +481,7 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
                     const float4 zb = lds4(zr + 4);                                // faces kb .. kb+3
                     const float zc = zr[8];                                        // face kb+4
                     // px[i] = 1 on x-interior planes, so min(px[i], min(py, pz)) = mpz there
-                    const float pxi = __ldg(a.tb.px + i);
+                    const float pxi = pxw;
                     float4 out;
                     out.x = pupd(cf, pown.x, qx2.x, qx1.x, qx3.x, qx0.x, yp.x, ym.x, ypp.x, ymm.x, zb.x, za.y, zb.y, za.x, fminf(pxi, mpz.x));
                     out.y = pupd(cf, pown.y, qx2.y, qx1.y, qx3.y, qx0.y, yp.y, ym.y, ypp.y, ymm.y, zb.y, zb.x, zb.z, za.y, fminf(pxi, mpz.y));
@@ -490,6 +497,8 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
             }
         }
 
+        axw3 = axw2; axw2 = axw1; axw1 = axw0; axw0 = ax_next;
+        pxw = px_next;
         // rotate: after it pslot[q] holds plane u+1-3+q and vslot[q] iteration u+1+q.
         // The slots receiving iteration u+D's loads (pslot[3+D-1], vslot[D-1]) were
         // freed one iteration ago: their last reads (plane u-4, iteration u-1)
