@@ -231,6 +231,23 @@ FDTD_B200_API int fdtd_b200_profile(AcousticFDTDState* st, int enable);
 FDTD_B200_API int fdtd_b200_profile_read(AcousticFDTDState* st, double* total_ms,
                                          long long* launches, long long* kernel_launches);
 
+/* No counterpart in the reference.  fdtd_sample_pressure_precomputed for
+ * callers that cannot allocate — a real-time audio callback sampling the
+ * microphones (an allocation may block on driver locks) or code recording a
+ * CUDA stream capture.  It never calls cudaMalloc/cudaFree or any allocating
+ * routine: its index/weight inputs and its results are staged in one fixed
+ * device array (272 KB, shared by all handles on a device and kept until the
+ * process exits).  At most 4096 receivers per call (FDTD_ERR_ARG beyond, with
+ * the reason in fdtd_b200_last_error).  The first call on a device looks up
+ * the array's device address; make that first call before any stream
+ * capture.  Each call overwrites what it uses of the array, so nothing in it
+ * has to start at zero, but calls that overlap on the GPU (other threads or
+ * streams) race on it.  Same arguments, indices checks and results as
+ * fdtd_sample_pressure_precomputed; returns after the values are in out_p. */
+FDTD_B200_API int fdtd_b200_sample_pressure_noalloc(const AcousticFDTDState* st, int n_rec,
+                                                   const int* idx8, const float* wgt8,
+                                                   float* out_p);
+
 /* Number of kernels this handle has launched since creation. */
 FDTD_B200_API long long fdtd_b200_launch_count(const AcousticFDTDState* st);
 

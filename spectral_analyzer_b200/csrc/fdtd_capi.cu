@@ -1335,3 +1335,92 @@ long long fdtd_b200_launch_count(const AcousticFDTDState* st) { return st ? st->
 const char* fdtd_b200_last_error(void) { return g_err; }
 
 }  // extern "C"
+
+/* ================= allocation-free pressure sampler ================= */
+/*
+ * Some callers cannot allocate: the instrument co-evolver samples its
+ * microphones once per audio sample from a real-time audio callback, where a
+ * cudaMalloc/cudaMallocHost may block on driver locks for an unbounded time,
+ * and a caller that is recording a CUDA stream capture may not allocate at
+ * all.  fdtd_sample_pressure_precomputed grows per-handle scratch on demand;
+ * this variant stages its inputs and result in one fixed device array instead.
+ */
+namespace {
+
+constexpr int kNoAllocMaxReceivers = 4096;   // receivers per call (8 taps each)
+
+struct NoAllocScratch {
+    int idx[kNoAllocMaxReceivers * 8];
+    float wgt[kNoAllocMaxReceivers * 8];
+    float out[kNoAllocMaxReceivers];
+};
+
+// 272 KB on every device that loads this library, held until the process exits.
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// Same sum as k_wsum for the precomputed sampler (products in tap order, the
+// first one starting the running sum), with the reference's flat indices
+// turned into device offsets here rather than on the host.
+__global__ void k_sample_noalloc(NoAllocScratch* s, const float* __restrict__ p, Grid g, int n_rec)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rec) return;
+    float acc = 0.0f;
+    for (int t = 0; t < 8; ++t) {
+        const int flat = s->idx[8 * r + t];   // validated in [0, N) on the host
+        const int k = flat % g.nz;
+        const int ij = flat / g.nz;
+        const long long off = ((long long)(ij / g.ny) * g.ny + ij % g.ny) * g.sz + k;
+        const float v = fmul(s->wgt[8 * r + t], p[off]);
+        acc = t == 0 ? v : fadd(acc, v);
+    }
+    s->out[r] = acc;
+}
+
+std::mutex g_noalloc_mu;
+NoAllocScratch* g_noalloc_addr[64];   // device address of the array, per device
+
+}  // namespace
+
+extern "C" int fdtd_b200_sample_pressure_noalloc(const AcousticFDTDState* cst, int n_rec,
+                                                 const int* idx8, const float* wgt8, float* out_p)
+{
+    AcousticFDTDState* st = const_cast<AcousticFDTDState*>(cst);
+    if (!st || !idx8 || !wgt8 || !out_p) return FDTD_ERR_NULL;
+    if (n_rec <= 0) return FDTD_OK;
+    if (n_rec > kNoAllocMaxReceivers) {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        snprintf(g_err, sizeof(g_err),
+                 "fdtd_b200_sample_pressure_noalloc: %d receivers exceed the maximum of %d per call",
+                 n_rec, kNoAllocMaxReceivers);
+        return FDTD_ERR_ARG;
+    }
+    for (long long q = 0; q < (long long)n_rec * 8; ++q)
+        if (idx8[q] < 0 || idx8[q] >= st->N) return FDTD_ERR_ARG;
+    if (dev_guard(st)) return FDTD_ERR_CUDA;
+    if (st->device < 0 || st->device >= 64) return FDTD_ERR_ARG;
+    NoAllocScratch* s;
+    {
+        // first call on this device (its device current): look up the array's address
+        std::lock_guard<std::mutex> lk(g_noalloc_mu);
+        if (!g_noalloc_addr[st->device]) {
+            void* addr = nullptr;
+            cudaError_t e = cudaGetSymbolAddress(&addr, g_noalloc_scratch);
+            if (e != cudaSuccess) {
+                set_err(e, "cudaGetSymbolAddress(g_noalloc_scratch)");
+                return FDTD_ERR_CUDA;
+            }
+            g_noalloc_addr[st->device] = static_cast<NoAllocScratch*>(addr);
+        }
+        s = g_noalloc_addr[st->device];
+    }
+    const size_t taps = (size_t)n_rec * 8;
+    CK(cudaMemcpyAsync(s->idx, idx8, taps * sizeof(int), cudaMemcpyHostToDevice, st->stream));
+    CK(cudaMemcpyAsync(s->wgt, wgt8, taps * sizeof(float), cudaMemcpyHostToDevice, st->stream));
+    k_sample_noalloc<<<(n_rec + 127) / 128, 128, 0, st->stream>>>(s, st->P(), st->g, n_rec);
+    CK(cudaGetLastError());
+    ++st->launches;
+    CK(cudaMemcpyAsync(out_p, s->out, (size_t)n_rec * sizeof(float), cudaMemcpyDeviceToHost, st->stream));
+    CK(cudaStreamSynchronize(st->stream));
+    return FDTD_OK;
+}
