@@ -60,6 +60,14 @@ def parse_args():
                     help="bound on the timed part of --impl reference")
     ap.add_argument("--grid", default=None,
                     help="NX,NY,NZ: a smaller seeded room of the same kind (profiling only)")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving benchmark: continuous batching vs sequential plain launches")
+    ap.add_argument("--serve-requests", type=int, default=256)
+    ap.add_argument("--serve-load", type=float, default=1.5,
+                    help="offered load as a multiple of the sequential plain capacity")
+    ap.add_argument("--serve-slots", type=int, default=64)
+    ap.add_argument("--serve-chunk", type=int, default=64)
+    ap.add_argument("--serve-max-steps", type=int, default=8000)
     args = ap.parse_args()
     global GRID
     GRID = tuple(int(v) for v in args.grid.split(",")) if args.grid else None
@@ -381,10 +389,49 @@ def engine_arm(args):
     return 0
 
 
+def serve_arm(args):
+    """Config-3 serving: Poisson arrivals at serve-load x the sequential capacity."""
+    import torch
+    from spectral_analyzer_b200 import autotune
+    from spectral_analyzer_b200.serving import (BatchServer, SequentialServer, calibrate_sequential,
+                                                config3_requests, poisson_arrivals, request_work,
+                                                summarize)
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    reqs = config3_requests(args.serve_requests, seed=3, steps=(500, args.serve_max_steps))
+    tune = autotune.tune_segment()
+    sample = reqs[:: max(1, len(reqs) // 16)]
+    service = calibrate_sequential(sample)
+    rate = args.serve_load / service
+    for r, t in zip(reqs, poisson_arrivals(len(reqs), rate, seed=5)):
+        r.arrival = float(t)
+    work = request_work(reqs)
+    seq = SequentialServer().run(reqs)
+    srv = BatchServer(max_slots=args.serve_slots, chunk=args.serve_chunk, seg_planes=tune["segment"])
+    bat = srv.run(reqs)
+    same = all(np.array_equal(a.traces.view(np.uint32), b.traces.view(np.uint32)) for a, b in zip(seq, bat))
+    s_seq, s_bat = summarize(seq, work), summarize(bat, work)
+    line = {"metric": "serve requests/s", "value": s_bat["requests_per_s"], "unit": "requests/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "config3_rooms", "requests": len(reqs), "axes": "32..256 step 16",
+                       "steps": [500, args.serve_max_steps], "receivers": "1..4",
+                       "arrivals": "poisson", "offered_load_x_sequential": args.serve_load,
+                       "arrival_rate_per_s": rate, "sequential_mean_service_s": service,
+                       "slots": args.serve_slots, "chunk_steps": args.serve_chunk,
+                       "segment_planes": tune["segment"]},
+            "batched": s_bat, "sequential": s_seq,
+            "speedup_requests_per_s": s_bat["requests_per_s"] / s_seq["requests_per_s"],
+            "traces_bit_identical": same, "max_rel_l2_vs_sequential": 0.0 if same else None,
+            "autotune": tune}
+    print(json.dumps(line), flush=True)
+    return 0 if same else 1
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.serve:
+        return serve_arm(args)
     return engine_arm(args)
 
 

@@ -248,6 +248,35 @@ FDTD_B200_API int fdtd_b200_sample_pressure_noalloc(const AcousticFDTDState* st,
                                                    const int* idx8, const float* wgt8,
                                                    float* out_p);
 
+/* ---- batched stepping of independent rooms (serving) ----
+ * A batch advances several solver handles together: each batched step is one
+ * persistent kernel over the work items (tile x plane segment) of every member
+ * below its step limit, plus one epilogue kernel (receivers, step counters,
+ * 256-step check, next source sample).  Members must be open rooms (no walls,
+ * fractions or active plate).  A member's arithmetic is the same as in
+ * fdtd_step, so its fields and traces are bit-identical alone and in a batch.
+ * Do not call other functions on a member while the batch holds it: take it
+ * out with fdtd_b200_batch_set (which first writes every member's progress
+ * back to its handle) or read its progress with fdtd_b200_batch_sync. */
+typedef struct FdtdB200Batch FdtdB200Batch;
+FDTD_B200_API FdtdB200Batch* fdtd_b200_batch_create(int device);
+FDTD_B200_API void fdtd_b200_batch_destroy(FdtdB200Batch* b);
+/* Replace the members; member q advances until its step count reaches limits[q]. */
+FDTD_B200_API int fdtd_b200_batch_set(FdtdB200Batch* b, AcousticFDTDState* const* members,
+                                      const int* limits, int n);
+/* Planes per work item (0 = automatic); takes effect at the next batch_set. */
+FDTD_B200_API int fdtd_b200_batch_set_segment(FdtdB200Batch* b, int planes);
+/* Launch n_steps batched steps without waiting; use_graph = 1 captures them
+ * once as a CUDA graph per n_steps and replays it (the graph stays valid
+ * across member sets; it is re-captured only when a set outgrows the
+ * descriptor capacity). */
+FDTD_B200_API int fdtd_b200_batch_step(FdtdB200Batch* b, int n_steps, int use_graph);
+/* Wait, then write each member's step count, buffers and traces back to its
+ * handle; steps_out[q] = step count, status_out[q] = 0 or FDTD_ERR_UNSTABLE
+ * (a failed 256-step check, latched; the member kept stepping). */
+FDTD_B200_API int fdtd_b200_batch_sync(FdtdB200Batch* b, int* steps_out, int* status_out);
+FDTD_B200_API long long fdtd_b200_batch_launch_count(const FdtdB200Batch* b);
+
 /* Number of kernels this handle has launched since creation. */
 FDTD_B200_API long long fdtd_b200_launch_count(const AcousticFDTDState* st);
 

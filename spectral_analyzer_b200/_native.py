@@ -68,6 +68,13 @@ SIGNATURES = {
     "fdtd_b200_profile_read": (i32, [vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong),
                                       C.POINTER(C.c_longlong)]),
     "fdtd_b200_sample_pressure_noalloc": (i32, [vp, i32, P_i32, P_f32, P_f32]),
+    "fdtd_b200_batch_create": (vp, [i32]),
+    "fdtd_b200_batch_destroy": (None, [vp]),
+    "fdtd_b200_batch_set": (i32, [vp, C.POINTER(vp), P_i32, i32]),
+    "fdtd_b200_batch_set_segment": (i32, [vp, i32]),
+    "fdtd_b200_batch_step": (i32, [vp, i32, i32]),
+    "fdtd_b200_batch_sync": (i32, [vp, P_i32, P_i32]),
+    "fdtd_b200_batch_launch_count": (C.c_longlong, [vp]),
     "fdtd_b200_launch_count": (C.c_longlong, [vp]),
     "fdtd_b200_last_error": (C.c_char_p, []),
 }

@@ -1,0 +1,82 @@
+"""Autotuner for the batched step's work-item shape.
+
+A work item of the batched kernel is one CTA tile (8 rows x 128 columns,
+fixed at compile time) marching a segment of planes.  Short segments give
+more items (better balance across SMs for uneven batches) but repeat the
+segment warm-up (3 extra planes in, 2 out per segment); long segments do the
+opposite.  ``tune_segment`` times the batched step on a calibration mix of
+rooms for each candidate depth (0 = one wave of items per room) and returns
+the fastest.  Results are cached per GPU name in a JSON file next to this
+module (or at ``$FDTD_B200_TUNE_CACHE``).
+"""
+from __future__ import annotations
+
+import json
+import os
+import time
+from typing import Dict, Optional, Sequence
+
+CANDIDATES = (0, 16, 32, 64, 128)
+CACHE = os.environ.get("FDTD_B200_TUNE_CACHE",
+                       os.path.join(os.path.dirname(os.path.abspath(__file__)), "_tuned.json"))
+
+
+def _gpu_key() -> str:
+    import torch
+    return torch.cuda.get_device_name(torch.cuda.current_device())
+
+
+def _load() -> Dict[str, dict]:
+    try:
+        with open(CACHE) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def calibration_rooms(n: int = 12, seed: int = 21):
+    from .serving import config3_requests
+    return [r.room for r in config3_requests(n, seed=seed, steps=(200, 200))]
+
+
+def time_segment(rooms, planes: int, steps: int = 64, reps: int = 3) -> float:
+    """Seconds per batched step of the calibration mix with the given depth."""
+    import torch
+    from .serving import EngineBatch, make_solver
+    solvers = [make_solver(r) for r in rooms]
+    b = EngineBatch()
+    b.set_segment(planes)
+    b.set(solvers, [10 ** 9] * len(solvers))
+    b.step(steps, True)          # capture + warm up
+    b.sync()
+    best = float("inf")
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        b.step(steps, True)
+        b.sync()
+        best = min(best, (time.perf_counter() - t0) / steps)
+    b.set([], [])
+    for s in solvers:
+        s.close()
+    del b
+    torch.cuda.synchronize()
+    return best
+
+
+def tune_segment(rooms=None, candidates: Sequence[int] = CANDIDATES, use_cache: bool = True) -> dict:
+    key = _gpu_key()
+    cache = _load()
+    if use_cache and key in cache and "segment" in cache[key]:
+        return cache[key]
+    rooms = rooms or calibration_rooms()
+    timings = {int(p): time_segment(rooms, int(p)) for p in candidates}
+    best = min(timings, key=timings.get)
+    entry = {"segment": best, "timings_s_per_step": timings,
+             "cells": int(sum(r.cells for r in rooms))}
+    cache[key] = entry
+    try:
+        with open(CACHE, "w") as f:
+            json.dump(cache, f, indent=1)
+    except OSError:
+        pass
+    return entry

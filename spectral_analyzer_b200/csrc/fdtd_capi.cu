@@ -121,6 +121,7 @@ struct AcousticFDTDState {
     float* d_ps_sig = nullptr;
     int ps_n = 0;
     int ps_cell = -1;
+    int ps_done_step = -1;           // step whose source sample is already in P
 
     // receivers
     int n_rec = 0;
@@ -495,9 +496,10 @@ int one_step(AcousticFDTDState* st, bool sync_check)
 {
     cudaStream_t s = st->stream;
     // point source: deposit s[n] before step n (applies before the plate reads P)
-    if (st->ps_n > 0 && st->step_count < st->ps_n && st->ps.n > 0) {
+    if (st->ps_n > 0 && st->step_count < st->ps_n && st->ps.n > 0 && st->ps_done_step != st->step_count) {
         CK(launch_deposit(st->ps, st->d_ps_sig, st->step_count, 0.0f, st->P(), s));
         ++st->launches;
+        st->ps_done_step = st->step_count;
     }
 
     // plate step (acoustic_fdtd.cpp:984-1053)
@@ -1024,6 +1026,7 @@ int fdtd_reset(AcousticFDTDState* st)
     st->dev_ext_nonzero = false;
     st->step_count = 0;
     st->trace_len = 0;
+    st->ps_done_step = -1;
     return FDTD_OK;
 }
 
@@ -1182,6 +1185,7 @@ int fdtd_b200_set_point_source(AcousticFDTDState* st, int cell_index, const floa
     st->ps_n = 0;
     st->ps = Deposit{};
     st->ps_cell = -1;
+    st->ps_done_step = -1;
     if (n_signal <= 0 || !signal) return FDTD_OK;
     if (cell_index < 0 || cell_index >= st->N) return FDTD_ERR_ARG;
     CK(cudaMalloc(&st->d_ps_sig, sizeof(float) * n_signal));
@@ -1424,3 +1428,294 @@ extern "C" int fdtd_b200_sample_pressure_noalloc(const AcousticFDTDState* cst, i
     CK(cudaStreamSynchronize(st->stream));
     return FDTD_OK;
 }
+
+/* ====================== batched stepping (continuous batching) ====================== */
+
+struct FdtdB200Batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<AcousticFDTDState*> members;
+    std::vector<BatchMember> h;          // host copy of the device descriptors
+    std::vector<int> cur0, cv0;          // member buffer parities when the batch was set
+    BatchMember* d_members = nullptr;
+    int cap_members = 0;
+    int* d_item_member = nullptr;
+    int cap_items = 0;
+    int total_items = 0;
+    BatchHeader* d_hdr = nullptr;
+    unsigned* d_status = nullptr;
+    unsigned h_status[kStatusWords];
+    int grid_ctas = 0;
+    int seg_planes = 0;                  // planes per work item, 0 = automatic
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    long long launches = 0;
+};
+
+namespace {
+
+void batch_drop_graph(FdtdB200Batch* b)
+{
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->graph_steps = 0;
+}
+
+// Pull the device step counters back into the member handles.
+int batch_pull(FdtdB200Batch* b, int* steps_out, int* status_out)
+{
+    const int n = (int)b->members.size();
+    if (n > 0)
+        CK(cudaMemcpyAsync(b->h.data(), b->d_members, sizeof(BatchMember) * n, cudaMemcpyDeviceToHost,
+                           b->stream));
+    CK(cudaMemcpyAsync(b->h_status, b->d_status, sizeof(b->h_status), cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    for (int q = 0; q < n; ++q) {
+        AcousticFDTDState* st = b->members[q];
+        const BatchMember& m = b->h[q];
+        const int done = m.step - m.step0;
+        st->step_count = m.step;
+        st->cur = b->cur0[q] ^ (done & 1);
+        st->cv = b->cv0[q] ^ (done & 1);
+        st->trace_len = std::min(m.trace0 + done, m.trace_cap);
+        const int n_chk = m.step / kCheckPeriod - m.step0 / kCheckPeriod;
+        st->stab_phase = (m.phase0 + n_chk) % kCheckStride;
+        if (m.step < m.limit && m.step < m.ps_n) st->ps_done_step = m.step;
+        if (steps_out) steps_out[q] = m.step;
+        if (status_out) status_out[q] = (m.unstable != 0xFFFFFFFFu) ? FDTD_ERR_UNSTABLE : FDTD_OK;
+    }
+    if (b->h_status[kStatusTimeout] != 0xFFFFFFFFu) {
+        std::lock_guard<std::mutex> lk(g_err_mu);
+        snprintf(g_err, sizeof(g_err), "batched step: a tile's load wait timed out (block %u)",
+                 b->h_status[kStatusTimeout]);
+        return FDTD_ERR_CUDA;
+    }
+    return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+FdtdB200Batch* fdtd_b200_batch_create(int device)
+{
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    FdtdB200Batch* b = new FdtdB200Batch();
+    if (device < 0 && cudaGetDevice(&device) != cudaSuccess) { delete b; return nullptr; }
+    b->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&b->d_hdr, sizeof(BatchHeader)) != cudaSuccess ||
+        cudaMemset(b->d_hdr, 0, sizeof(BatchHeader)) != cudaSuccess ||
+        cudaMalloc(&b->d_status, sizeof(unsigned) * kStatusWords) != cudaSuccess ||
+        cudaMemset(b->d_status, 0xFF, sizeof(unsigned) * kStatusWords) != cudaSuccess ||
+        fused_batch_slots(&b->grid_ctas) != cudaSuccess) {
+        set_err(cudaGetLastError(), "fdtd_b200_batch_create");
+        fdtd_b200_batch_destroy(b);
+        return nullptr;
+    }
+    return b;
+}
+
+void fdtd_b200_batch_destroy(FdtdB200Batch* b)
+{
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_drop_graph(b);
+    cudaFree(b->d_members);
+    cudaFree(b->d_item_member);
+    cudaFree(b->d_hdr);
+    cudaFree(b->d_status);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+int fdtd_b200_batch_set_segment(FdtdB200Batch* b, int planes)
+{
+    if (!b) return FDTD_ERR_NULL;
+    if (planes < 0) return FDTD_ERR_ARG;
+    b->seg_planes = planes;
+    batch_drop_graph(b);
+    return FDTD_OK;
+}
+
+int fdtd_b200_batch_set(FdtdB200Batch* b, AcousticFDTDState* const* members, const int* limits, int n)
+{
+    if (!b || (n > 0 && (!members || !limits))) return FDTD_ERR_NULL;
+    if (n < 0) return FDTD_ERR_ARG;
+    CK(cudaSetDevice(b->device));
+    // the previous members' progress goes back to their handles first
+    if (!b->members.empty()) {
+        int rc = batch_pull(b, nullptr, nullptr);
+        if (rc) return rc;
+    }
+    b->members.clear();
+    b->h.clear();
+    b->cur0.clear();
+    b->cv0.clear();
+    b->total_items = 0;
+    if (n == 0) {
+        BatchHeader hz{0, 0, 0};
+        CK(cudaMemcpyAsync(b->d_hdr, &hz, sizeof(hz), cudaMemcpyHostToDevice, b->stream));
+        CK(cudaStreamSynchronize(b->stream));
+        return FDTD_OK;
+    }
+    for (int q = 0; q < n; ++q) {
+        AcousticFDTDState* st = members[q];
+        if (!st) return FDTD_ERR_NULL;
+        if (st->device != b->device || !fused_eligible(st) || limits[q] < st->step_count) return FDTD_ERR_ARG;
+    }
+    int tj, tk;
+    fused_tile_shape(&tj, &tk);
+    std::vector<int> item_member;
+    for (int q = 0; q < n; ++q) {
+        AcousticFDTDState* st = members[q];
+        CK(cudaStreamSynchronize(st->stream));
+        if (!st->v[st->cv ^ 1][0]) {
+            int rc = alloc_second_velocity_set(st);
+            if (rc) return rc;
+            CK(cudaStreamSynchronize(st->stream));
+        }
+        if (!st->fcache) st->fcache = fused_cache_create();
+        // the member's next source sample goes in before its first batched step
+        if (st->ps_n > 0 && st->step_count < st->ps_n && st->ps.n > 0 && st->ps_done_step != st->step_count &&
+            st->step_count < limits[q]) {
+            CK(launch_deposit(st->ps, st->d_ps_sig, st->step_count, 0.0f, st->P(), b->stream));
+            ++b->launches;
+            st->ps_done_step = st->step_count;
+        }
+        BatchMember m;
+        memset(&m, 0, sizeof(m));
+        const float* v0[3] = {st->V(0), st->V(1), st->V(2)};
+        const float* v1[3] = {st->v[st->cv ^ 1][0], st->v[st->cv ^ 1][1], st->v[st->cv ^ 1][2]};
+        CK(fused_maps(st->fcache, st->g, st->P(), v0, m.maps[0]));
+        CK(fused_maps(st->fcache, st->g, st->Pn(), v1, m.maps[1]));
+        m.g = st->g;
+        m.cf = st->cf;
+        m.tb = st->tb;
+        m.p[0] = st->P();
+        m.p[1] = st->Pn();
+        for (int c = 0; c < 3; ++c) {
+            m.v[0][c] = st->V(c);
+            m.v[1][c] = st->v[st->cv ^ 1][c];
+        }
+        m.step = m.step0 = st->step_count;
+        m.limit = limits[q];
+        const int tiles_j = (st->Ny + tj - 1) / tj, tiles_k = (st->Nz + tk - 1) / tk;
+        m.tiles_k = tiles_k;
+        m.tiles = tiles_j * tiles_k;
+        int segs;
+        if (b->seg_planes > 0) {
+            segs = (st->Nx + b->seg_planes - 1) / b->seg_planes;
+        } else {
+            // automatic: about one wave of work items for this member alone
+            segs = std::max(1, b->grid_ctas / m.tiles);
+        }
+        segs = std::min(segs, st->Nx);
+        m.seg_len = (st->Nx + segs - 1) / segs;
+        segs = (st->Nx + m.seg_len - 1) / m.seg_len;
+        m.items_begin = (int)item_member.size();
+        for (int t = 0; t < m.tiles * segs; ++t) item_member.push_back(q);
+        m.ps = st->ps;
+        m.ps_sig = st->d_ps_sig;
+        m.ps_n = (st->ps.n > 0 && st->d_ps_sig) ? st->ps_n : 0;
+        m.n_rec = st->n_rec;
+        m.trace0 = st->trace_len;
+        m.trace_cap = st->trace_cap;
+        m.rec_idx = st->d_rec_idx;
+        m.rec_w = st->d_rec_w;
+        m.trace = st->d_trace;
+        m.n_cells = st->N;
+        m.phase0 = st->stab_phase;
+        m.unstable = 0xFFFFFFFFu;
+        b->members.push_back(st);
+        b->h.push_back(m);
+        b->cur0.push_back(st->cur);
+        b->cv0.push_back(st->cv);
+    }
+    // descriptor arrays keep their addresses (and a captured graph stays valid)
+    // until a set outgrows them
+    if (n > b->cap_members) {
+        batch_drop_graph(b);
+        cudaFree(b->d_members);
+        b->d_members = nullptr;
+        b->cap_members = 0;
+        const int cap = std::max(n, std::max(64, 2 * b->cap_members));
+        CK(cudaMalloc(&b->d_members, sizeof(BatchMember) * cap));
+        b->cap_members = cap;
+    }
+    if ((int)item_member.size() > b->cap_items) {
+        batch_drop_graph(b);
+        cudaFree(b->d_item_member);
+        b->d_item_member = nullptr;
+        b->cap_items = 0;
+        const int cap = std::max((int)item_member.size(), 1 << 15);
+        CK(cudaMalloc(&b->d_item_member, sizeof(int) * cap));
+        b->cap_items = cap;
+    }
+    b->total_items = (int)item_member.size();
+    BatchHeader hh{n, b->total_items, 0};
+    CK(cudaMemcpyAsync(b->d_members, b->h.data(), sizeof(BatchMember) * n, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaMemcpyAsync(b->d_item_member, item_member.data(), sizeof(int) * item_member.size(),
+                       cudaMemcpyHostToDevice, b->stream));
+    CK(cudaMemcpyAsync(b->d_hdr, &hh, sizeof(hh), cudaMemcpyHostToDevice, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    return FDTD_OK;
+}
+
+int fdtd_b200_batch_step(FdtdB200Batch* b, int n_steps, int use_graph)
+{
+    if (!b) return FDTD_ERR_NULL;
+    if (n_steps <= 0 || b->members.empty()) return FDTD_OK;
+    CK(cudaSetDevice(b->device));
+    if (!use_graph) {
+        for (int s = 0; s < n_steps; ++s) {
+            CK(launch_fused_batch_step(b->d_members, b->d_hdr, b->d_item_member, b->d_status,
+                                       b->grid_ctas, b->cap_members, b->stream));
+            b->launches += 2;
+        }
+        return FDTD_OK;
+    }
+    if (!b->graph || b->graph_steps != n_steps) {
+        batch_drop_graph(b);
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+        cudaError_t e = cudaSuccess;
+        for (int s = 0; s < n_steps && e == cudaSuccess; ++s)
+            e = launch_fused_batch_step(b->d_members, b->d_hdr, b->d_item_member, b->d_status,
+                                        b->grid_ctas, b->cap_members, b->stream);
+        cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
+        if (e != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            set_err(e != cudaSuccess ? e : e2, "batch graph capture");
+            return FDTD_ERR_CUDA;
+        }
+        e = cudaGraphInstantiate(&b->graph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            b->graph = nullptr;
+            set_err(e, "cudaGraphInstantiate");
+            return FDTD_ERR_CUDA;
+        }
+        b->graph_steps = n_steps;
+    }
+    CK(cudaGraphLaunch(b->graph, b->stream));
+    b->launches += 2LL * n_steps;
+    return FDTD_OK;
+}
+
+int fdtd_b200_batch_sync(FdtdB200Batch* b, int* steps_out, int* status_out)
+{
+    if (!b) return FDTD_ERR_NULL;
+    CK(cudaSetDevice(b->device));
+    return batch_pull(b, steps_out, status_out);
+}
+
+long long fdtd_b200_batch_launch_count(const FdtdB200Batch* b) { return b ? b->launches : 0; }
+
+}  // extern "C"

@@ -198,34 +198,80 @@ __device__ __forceinline__ float pupd(const Coef& cf, float p, float xp, float x
     return fmul(fsub(p, fmul(cf.bulk, dv)), pd);
 }
 
+// Load-pipeline state carried by a CTA from one tile to the next: rotating slot
+// ids and the mbarrier parity to wait for next, per slot.  Between tiles every
+// issued load has been consumed, so pslot[3 .. 3+D] and vslot[0 .. D] are free.
 template <class C>
-__global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
-                                                      const __grid_constant__ CUtensorMap tmP,
-                                                      const __grid_constant__ CUtensorMap tmX,
-                                                      const __grid_constant__ CUtensorMap tmY,
-                                                      const __grid_constant__ CUtensorMap tmZ,
-                                                      int seg_len, int tiles_k)
+struct Pipe {
+    int pslot[C::RING];
+    int vslot[C::VSTAGES];
+    unsigned pph, vph;
+    __device__ void init()
+    {
+#pragma unroll
+        for (int q = 0; q < C::RING; ++q) pslot[q] = q;
+#pragma unroll
+        for (int q = 0; q < C::VSTAGES; ++q) vslot[q] = q;
+        pph = vph = 0;
+    }
+};
+
+template <class C>
+__device__ __forceinline__ unsigned smem_base_u32(float** smem_out)
 {
     extern __shared__ float smem_raw[];
     float* const smem = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(smem_raw) + 127) & ~uintptr_t(127));
+    *smem_out = smem;
+    return smem_u32(smem);
+}
+
+template <class C>
+__device__ __forceinline__ void init_barriers(unsigned bar0)
+{
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < C::RING + C::VSTAGES; ++q) mbar_init(bar0 + 8u * q, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+    }
+    __syncthreads();
+}
+
+// One tile (TJ x TK columns, planes [seg*seg_len, ...)) of the fused step.
+// Returns false when a load wait ran out (the CTA must stop; status is set).
+// Make the tensor map at `map` (in global memory, rewritten by a host copy since
+// it was last used) visible to the TMA unit instead of a cached older copy.
+__device__ __forceinline__ void acquire_tensormap(const CUtensorMap* map)
+{
+    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(map) : "memory");
+}
+
+template <class C>
+__device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap* tmP,
+                                           const CUtensorMap* tmX, const CUtensorMap* tmY,
+                                           const CUtensorMap* tmZ, int tile, int seg, int seg_len,
+                                           int tiles_k, float* smem, unsigned sbase, unsigned bar0,
+                                           Pipe<C>& pp, bool acquire_maps = false)
+{
     float* const vyn = smem + C::VYN0;
     float* const vzn = smem + C::VZN0;
     float* const ay_s = smem + C::AY0;
     float* const az_s = smem + C::AZ0;
-    const unsigned sbase = smem_u32(smem);
-    const unsigned bar0 = sbase + 4u * C::BAR0;   // P slot s: bar0 + 8s; V stage v: bar0 + 8(RING+v)
+    int* const pslot = pp.pslot;
+    int* const vslot = pp.vslot;
+    unsigned& pph = pp.pph;
+    unsigned& vph = pp.vph;
 
     const Grid g = a.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz, sz = g.sz;
     const long long PL = g.plane;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int tk = blockIdx.x % tiles_k, tj = blockIdx.x / tiles_k;
+    const int tk = tile % tiles_k, tj = tile / tiles_k;
     const int j0 = tj * C::TJ, k0 = tk * C::TK;
-    const int i_beg = blockIdx.y * seg_len;
-    if (i_beg >= nx) return;
+    const int i_beg = seg * seg_len;
+    if (i_beg >= nx) return true;
     const int i_end = min(i_beg + seg_len, nx);
     const Coef cf = a.cf;
 
+    __syncthreads();   // the previous tile's readers of the tables are done
     for (int e = tid; e < C::AY_N; e += C::NT) {
         const int j = j0 - 2 + e;
         ay_s[e] = (j >= 0 && j < ny) ? __ldg(a.tb.ay + j) : 0.0f;
@@ -233,10 +279,6 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
     for (int e = tid; e < C::PC; e += C::NT) {
         const int k = k0 - 4 + e;
         az_s[e] = (k >= 0 && k < nz) ? __ldg(a.tb.az + k) : 0.0f;
-    }
-    if (tid == 0) {
-        for (int q = 0; q < C::RING + C::VSTAGES; ++q) mbar_init(bar0 + 8u * q, 1);
-        asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     __syncthreads();
 
@@ -247,31 +289,32 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         const unsigned pb = bar0 + 8u * ps;
         mbar_expect_tx(pb, C::P_BYTES);
-        tma_load3(sbase + 4u * (C::RING0 + ps * C::P_STAGE), &tmP, k0 - 4, j0 - 3, u, pb);
+        tma_load3(sbase + 4u * (C::RING0 + ps * C::P_STAGE), tmP, k0 - 4, j0 - 3, u, pb);
         const int f = u - 2, io = u - 3;
         const bool vx = (u >= i_beg && f >= 0 && f <= nx - 2);
         const bool vyz = (io >= i_beg && io < i_end);
         const unsigned vb = bar0 + 8u * (C::RING + vsg);
         const unsigned vdst = sbase + 4u * (C::VST0 + vsg * C::V_STAGE);
         mbar_expect_tx(vb, (vx ? C::VX_BYTES : 0u) + (vyz ? C::VYZ_BYTES : 0u));
-        if (vx) tma_load3(vdst + 4u * C::VX_OFF, &tmX, k0, j0, f, vb);
+        if (vx) tma_load3(vdst + 4u * C::VX_OFF, tmX, k0, j0, f, vb);
         if (vyz) {
-            tma_load3(vdst + 4u * C::VY_OFF, &tmY, k0, j0 - 2, io, vb);
-            tma_load3(vdst + 4u * C::VZ_OFF, &tmZ, k0 - 4, j0, io, vb);
+            tma_load3(vdst + 4u * C::VY_OFF, tmY, k0, j0 - 2, io, vb);
+            tma_load3(vdst + 4u * C::VZ_OFF, tmZ, k0 - 4, j0, io, vb);
         }
     };
 
+    if (acquire_maps && tid == 0) {
+        acquire_tensormap(tmP);
+        acquire_tensormap(tmX);
+        acquire_tensormap(tmY);
+        acquire_tensormap(tmZ);
+    }
     const int u0 = i_beg - 3, u1 = i_end + 2;
     // Slot ids, rotated each iteration.  At iteration u: pslot[0..3] hold planes
     // u-3 .. u, pslot[4 .. 3+D-1] planes u+1 .. u+D-1 in flight, pslot[3+D] is
     // free; vslot[0] holds iteration u's V data, vslot[1 .. D-1] the next
     // iterations' in flight, vslot[D] is free.  pph/vph: parity to wait for, per slot.
-    int pslot[C::RING], vslot[C::VSTAGES];
-#pragma unroll
-    for (int q = 0; q < C::RING; ++q) pslot[q] = q;
-#pragma unroll
-    for (int q = 0; q < C::VSTAGES; ++q) vslot[q] = q;
-    unsigned pph = 0, vph = 0;
+    // The first D iterations' loads go into the free slots left by the previous tile.
     if (tid == 0)
         for (int q = 0; q < C::D; ++q) issue(u0 + q, pslot[3 + q], vslot[q]);
 
@@ -520,12 +563,123 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
     // After a timed-out wait at iteration u_fail, the copies issued for
     // iterations u_fail .. u_fail+D-1 may still be landing: wait for them
     // (bounded) before the CTA's shared memory is released.
-    if (u_fail <= u1 && tid == 0) {
-        for (int q = 0; q < C::D && u_fail + q <= u1; ++q) {
-            const int ps = pslot[3 + q], vsg = vslot[q];
-            mbar_wait(bar0 + 8u * ps, (pph >> ps) & 1u);
-            mbar_wait(bar0 + 8u * (C::RING + vsg), (vph >> vsg) & 1u);
+    if (u_fail <= u1) {
+        if (tid == 0) {
+            for (int q = 0; q < C::D && u_fail + q <= u1; ++q) {
+                const int ps = pslot[3 + q], vsg = vslot[q];
+                mbar_wait(bar0 + 8u * ps, (pph >> ps) & 1u);
+                mbar_wait(bar0 + 8u * (C::RING + vsg), (vph >> vsg) & 1u);
+            }
         }
+        __syncthreads();
+        return false;
+    }
+    return true;
+}
+
+// Single-room step: one CTA per (tile, segment).
+template <class C>
+__global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
+                                                      const __grid_constant__ CUtensorMap tmP,
+                                                      const __grid_constant__ CUtensorMap tmX,
+                                                      const __grid_constant__ CUtensorMap tmY,
+                                                      const __grid_constant__ CUtensorMap tmZ,
+                                                      int seg_len, int tiles_k)
+{
+    if ((int)blockIdx.y * seg_len >= a.g.nx) return;
+    float* smem;
+    const unsigned sbase = smem_base_u32<C>(&smem);
+    const unsigned bar0 = sbase + 4u * C::BAR0;
+    init_barriers<C>(bar0);
+    Pipe<C> pp;
+    pp.init();
+    fused_tile<C>(a, &tmP, &tmX, &tmY, &tmZ, blockIdx.x, blockIdx.y, seg_len, tiles_k, smem, sbase,
+                  bar0, pp);
+}
+
+
+// Batched step: a persistent kernel whose CTAs pull (member, tile, segment)
+// work items from a device counter until the list is exhausted; members at
+// their step limit are skipped.  Uneven members balance across the SMs.  The
+// members' tensor maps live in global memory and are rewritten when the set
+// changes, so each work item acquires them before its first TMA load.
+template <class C>
+__global__ void __launch_bounds__(C::NT, 2) k_fused_batch(BatchMember* __restrict__ mem,
+                                                          BatchHeader* __restrict__ hdr,
+                                                          const int* __restrict__ item_member,
+                                                          unsigned* __restrict__ status)
+{
+    __shared__ int s_item;
+    const int total_items = hdr->total_items;
+    int* const counter = &hdr->counter;
+    float* smem;
+    const unsigned sbase = smem_base_u32<C>(&smem);
+    const unsigned bar0 = sbase + 4u * C::BAR0;
+    init_barriers<C>(bar0);
+    Pipe<C> pp;
+    pp.init();
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        __syncthreads();
+        if (item >= total_items) break;
+        const BatchMember* m = mem + item_member[item];
+        const int step = m->step;
+        if (step >= m->limit) continue;
+        const int par = (step - m->step0) & 1;
+        FusedArgs a;
+        a.g = m->g;
+        a.cf = m->cf;
+        a.tb = m->tb;
+        a.p = m->p[par];
+        a.pn = m->p[par ^ 1];
+        for (int c = 0; c < 3; ++c) {
+            a.vin[c] = m->v[par][c];
+            a.vout[c] = m->v[par ^ 1][c];
+        }
+        a.status = status;
+        const int local = item - m->items_begin;
+        if (!fused_tile<C>(a, &m->maps[par][0], &m->maps[par][1], &m->maps[par][2], &m->maps[par][3],
+                           local % m->tiles, local / m->tiles, m->seg_len, m->tiles_k, smem, sbase,
+                           bar0, pp, true))
+            break;
+    }
+}
+
+// After a batched step, per member below its limit: record the receivers from
+// the new pressure, advance the step counter, run the 256-step check, then
+// deposit the next step's source sample (the order of the single-room path:
+// record after step n, deposit before step n+1).  One block per member.
+__global__ void k_batch_epilogue(BatchMember* __restrict__ mem, const BatchHeader* __restrict__ hdr)
+{
+    const int r = blockIdx.x;
+    if (r >= hdr->n_members) return;
+    BatchMember* m = mem + r;
+    const int s = m->step;
+    if (s >= m->limit) return;
+    const int s1 = s + 1;
+    float* P = m->p[(s1 - m->step0) & 1];
+    const int slot = m->trace0 + (s - m->step0);
+    if (slot < m->trace_cap)
+        for (int q = threadIdx.x; q < m->n_rec; q += blockDim.x)
+            m->trace[(size_t)slot * m->n_rec + q] = sample8(P, m->rec_idx + 8 * q, m->rec_w + 8 * q);
+    if ((s1 & (kCheckPeriod - 1)) == 0) {
+        const int n_chk = s1 / kCheckPeriod - m->step0 / kCheckPeriod;
+        const long long phase = (m->phase0 + n_chk - 1) % kCheckStride;
+        const Grid g = m->g;
+        for (long long q = phase + (long long)kCheckStride * threadIdx.x; q < m->n_cells;
+             q += (long long)kCheckStride * blockDim.x) {
+            const int k = (int)(q % g.nz);
+            const long long ij = q / g.nz;
+            const float v = P[((ij / g.ny) * g.ny + ij % g.ny) * g.sz + k];
+            if (!isfinite(v) || v > 2e3f || v < -2e3f) atomicCAS(&m->unstable, 0xFFFFFFFFu, (unsigned)s1);
+        }
+    }
+    __syncthreads();   // receivers have read P before the deposit below changes it
+    if (threadIdx.x == 0) {
+        if (s1 < m->limit && s1 < m->ps_n) deposit_apply(m->ps, m->ps_sig[s1], P);
+        m->step = s1;
     }
 }
 
@@ -644,6 +798,54 @@ cudaError_t launch_fused_step(const FusedArgs& a, FusedCache* cache, cudaStream_
     dim3 grid((unsigned)tiles, (unsigned)segs, 1);
     k_fused_step<C><<<grid, C::NT, C::SMEM_BYTES, s>>>(a, maps[0], maps[1], maps[2], maps[3], seg_len,
                                                        tiles_k);
+    return cudaGetLastError();
+}
+
+cudaError_t fused_maps(FusedCache* c, const Grid& g, const float* p, const float* const* v,
+                       CUtensorMap out[4])
+{
+    const float* bases[4] = {p, v[0], v[1], v[2]};
+    for (int q = 0; q < 4; ++q) {
+        cudaError_t e = cached_map(c, bases[q], q, g, &out[q]);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+void fused_tile_shape(int* tj, int* tk)
+{
+    *tj = FusedCfg::TJ;
+    *tk = FusedCfg::TK;
+}
+
+cudaError_t fused_batch_slots(int* slots)
+{
+    using C = FusedCfg;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_fused_batch<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)C::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    int sms = 0, per = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fused_batch<C>, C::NT, C::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    *slots = (per > 0 ? per : 1) * sms;
+    return cudaSuccess;
+}
+
+cudaError_t launch_fused_batch_step(BatchMember* members, BatchHeader* hdr, const int* item_member,
+                                    unsigned* status, int grid_ctas, int epi_blocks, cudaStream_t s)
+{
+    using C = FusedCfg;
+    cudaError_t e = cudaMemsetAsync(&hdr->counter, 0, sizeof(int), s);
+    if (e != cudaSuccess) return e;
+    k_fused_batch<C><<<grid_ctas, C::NT, C::SMEM_BYTES, s>>>(members, hdr, item_member, status);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    k_batch_epilogue<<<epi_blocks, 128, 0, s>>>(members, hdr);
     return cudaGetLastError();
 }
 

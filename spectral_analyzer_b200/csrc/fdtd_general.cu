@@ -170,14 +170,7 @@ __global__ void k_plate_inject(int n_act, const int* __restrict__ act,
 __global__ void k_deposit(Deposit d, const float* __restrict__ signal, int step, float amp,
                           float* __restrict__ p)
 {
-    const float a = signal ? signal[step] : amp;
-    if (a == 0.0f || d.n == 0) return;
-    if (d.divisor == 0) {
-        p[d.idx[0]] = fadd(p[d.idx[0]], a);
-        return;
-    }
-    const float share = __fdiv_rn(a, (float)d.divisor);
-    for (int q = 0; q < d.n; ++q) p[d.idx[q]] = fadd(p[d.idx[q]], share);
+    deposit_apply(d, signal ? signal[step] : amp, p);
 }
 
 // out[r] = sum_t w[r*taps+t] * f[idx[r*taps+t]] in tap order; from_zero starts

@@ -17,6 +17,7 @@
  * results are bit-identical to the reference built without FMA contraction.
  */
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -80,6 +81,28 @@ __device__ __forceinline__ float face_damp(float aL, float aR, float dt)
     return fsub(1.0f, fmul(fmul(0.5f, fadd(aL, aR)), dt));
 }
 
+// One deposit of the open-cell rule (acoustic_fdtd.cpp:840-872); zero amplitude
+// is a no-op, a solid cell splits amp/m over its m open face neighbours.
+__device__ __forceinline__ void deposit_apply(const Deposit& d, float amp, float* p)
+{
+    if (amp == 0.0f || d.n == 0) return;
+    if (d.divisor == 0) {
+        p[d.idx[0]] = fadd(p[d.idx[0]], amp);
+        return;
+    }
+    const float share = __fdiv_rn(amp, (float)d.divisor);
+    for (int q = 0; q < d.n; ++q) p[d.idx[q]] = fadd(p[d.idx[q]], share);
+}
+
+// 8-tap precomputed sample (acoustic_fdtd.cpp:1673-1674): products in tap
+// order, the first one starting the running sum.
+__device__ __forceinline__ float sample8(const float* f, const long long* idx, const float* w)
+{
+    float s = fmul(w[0], f[idx[0]]);
+    for (int t = 1; t < 8; ++t) s = fadd(s, fmul(w[t], f[idx[t]]));
+    return s;
+}
+
 // ---- launchers (fdtd_general.cu) ----
 cudaError_t launch_velocity_general(const Grid& g, const Coef& cf, const Tables& tb,
                                     const float* p, float* vx, float* vy, float* vz,
@@ -120,5 +143,53 @@ void fused_cache_destroy(FusedCache* c);
 bool fused_supported(const Grid& g);
 cudaError_t launch_fused_step(const FusedArgs& a, FusedCache* cache, cudaStream_t s);
 int fused_kernel_launches_per_step();
+// TMA descriptors of the four fields a fused step reads (P, Vx, Vy, Vz).
+cudaError_t fused_maps(FusedCache* c, const Grid& g, const float* p, const float* const* v,
+                       CUtensorMap out[4]);
+
+// ---- batched step (continuous batching of independent rooms) ----
+// Device-resident descriptor of one batch member.  Parity 0 is the member's
+// state when it joined the batch; a step taken at parity q reads p[q], v[q]
+// and writes p[q^1], v[q^1].
+struct alignas(64) BatchMember {
+    CUtensorMap maps[2][4];      // per parity: P, Vx, Vy, Vz read by the step
+    Grid g;
+    Coef cf;
+    Tables tb;
+    float* p[2];
+    float* v[2][3];
+    int step;                    // device step counter (advanced by the epilogue)
+    int step0, limit;            // step count on joining; stop at this step count
+    int items_begin, tiles, tiles_k, seg_len;
+    // point source
+    Deposit ps;
+    const float* ps_sig;
+    int ps_n;
+    // receivers
+    int n_rec, trace0, trace_cap;
+    const long long* rec_idx;
+    const float* rec_w;
+    float* trace;
+    // stability check
+    int n_cells, phase0;
+    unsigned unstable;           // first step whose check failed (0xFFFFFFFF = none)
+};
+// Tile geometry of the fused step: rows x columns of a tile.
+void fused_tile_shape(int* tj, int* tk);
+// Resident CTAs of the batched kernel on the current device (all SMs).
+cudaError_t fused_batch_slots(int* slots);
+// Sizes of the current member set, read by the kernels from device memory so
+// that a captured graph stays valid when the set changes.
+struct BatchHeader {
+    int n_members;
+    int total_items;
+    int counter;                 // work-item counter, reset before each step
+};
+// One batched step: every member below its limit advances one step (fused
+// velocity+pressure over item_member's work items, then the epilogue:
+// receivers, step counter, 256-step check, next source sample).  epi_blocks
+// is the member capacity (blocks beyond n_members exit at once).
+cudaError_t launch_fused_batch_step(BatchMember* members, BatchHeader* hdr, const int* item_member,
+                                    unsigned* status, int grid_ctas, int epi_blocks, cudaStream_t s);
 
 }  // namespace fdtd

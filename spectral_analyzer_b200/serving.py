@@ -1,0 +1,302 @@
+"""Serving rooms: continuous batching of independent FDTD requests on one GPU.
+
+A request is a room (grid, absorption, point source, receivers, step count);
+its result is the receivers' traces.  ``BatchServer`` admits requests as they
+arrive, whenever a slot and device memory are free, and advances all admitted
+rooms together with the engine's batched step (one persistent kernel over the
+work items of every room per time step, plus a small epilogue), replaying a
+CUDA graph of ``chunk`` steps between scheduling points.  Rooms finish
+independently and leave the batch at the next chunk boundary; newly arrived
+rooms join there.  ``SequentialServer`` is the baseline: one request at a time
+through the plain single-room path.
+
+Both compute each room with the same arithmetic, so a room's traces are
+bit-identical alone and in any mix of other rooms.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from collections import deque
+from dataclasses import dataclass, field
+from typing import Callable, Dict, List, Optional, Sequence
+
+import numpy as np
+
+from .rooms import Room, reference_dt
+
+GRID_AXES = tuple(range(32, 257, 16))
+
+
+@dataclass
+class Request:
+    rid: int
+    room: Room
+    arrival: float = 0.0        # seconds after the start of the run
+
+
+@dataclass
+class Result:
+    rid: int
+    traces: np.ndarray          # (steps, n_rec) float32
+    arrival: float
+    start: float
+    finish: float
+
+    @property
+    def latency(self) -> float:
+        return self.finish - self.arrival
+
+
+def room_bytes(room: Room) -> int:
+    """Device memory of one room: 8 fields (P x2, V x2 sets) plus its trace."""
+    sz = (room.nz + 7) // 8 * 8
+    return 8 * room.nx * room.ny * sz * 4 + room.n_steps * len(room.receivers) * 4 + (1 << 16)
+
+
+def config3_requests(n: int = 256, seed: int = 3, steps=(500, 8000), axes=GRID_AXES,
+                     rec=(1, 4), a_range=(0.02, 0.3), n_pml: int = 10) -> List[Request]:
+    """Rooms with axes drawn from ``axes``, steps U{steps}, 1-4 receivers, per-face
+    absorption U[a_range], Gaussian or Ricker source, interior source/receivers."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for q in range(n):
+        nx, ny, nz = (int(rng.choice(axes)) for _ in range(3))
+        n_steps = int(rng.integers(steps[0], steps[1] + 1))
+        n_rec = int(rng.integers(rec[0], rec[1] + 1))
+        a6 = tuple(float(v) for v in rng.uniform(a_range[0], a_range[1], 6).astype(np.float32))
+        kind = "gaussian" if rng.random() < 0.5 else "ricker"
+
+        def interior(d):
+            lo, hi = n_pml + 2, d - n_pml - 2
+            return int(rng.integers(lo, hi)) if lo < hi else d // 2
+
+        src = (interior(nx), interior(ny), interior(nz))
+        recs = [(interior(nx), interior(ny), interior(nz)) for _ in range(n_rec)]
+        room = Room(nx, ny, nz, n_steps, src, recs, a6, kind, n_pml=n_pml, name=f"req{q}")
+        out.append(Request(q, room))
+    return out
+
+
+def poisson_arrivals(n: int, rate: float, seed: int = 5) -> np.ndarray:
+    """Arrival times (s) of a Poisson process with the given rate (requests/s)."""
+    rng = np.random.default_rng(seed)
+    return np.cumsum(rng.exponential(1.0 / rate, size=n))
+
+
+def percentile(xs: Sequence[float], p: float) -> float:
+    return float(np.percentile(np.asarray(xs, dtype=np.float64), p)) if len(xs) else float("nan")
+
+
+def summarize(results: Sequence[Result], work: float) -> dict:
+    lat = [r.latency for r in results]
+    t_first = min(r.arrival for r in results)
+    t_last = max(r.finish for r in results)
+    span = t_last - t_first
+    return {"requests": len(results), "makespan_s": span, "requests_per_s": len(results) / span,
+            "p50_latency_s": percentile(lat, 50), "p99_latency_s": percentile(lat, 99),
+            "mean_latency_s": float(np.mean(lat)), "gcell_updates_per_s": work / span / 1e9}
+
+
+def request_work(reqs: Sequence[Request]) -> float:
+    return float(sum(r.room.cells * r.room.n_steps for r in reqs))
+
+
+# ---------------------------------------------------------------- engine glue
+def make_solver(room: Room, device=None):
+    """A single-room solver configured for a request (source and receivers set)."""
+    from .fdtd import AcousticFDTD
+    f = AcousticFDTD(room.nx, room.ny, room.nz, room.dx, room.c, room.rho,
+                     cell_type=room.cell_type(), plate_iz=-1, plate_active=room.plate_active(),
+                     n_pml=room.n_pml, device=device)
+    f.set_face_absorption(room.absorption)
+    idx, w = f.precompute_pressure_samplers(room.receiver_xyz())
+    f.set_point_source(room.src_flat, room.signal())
+    f.set_receivers(idx, w, room.n_steps)
+    return f
+
+
+class EngineBatch:
+    """ctypes wrapper of the engine's batch object (fdtd_b200_batch_*)."""
+
+    def __init__(self, device: int = 0):
+        from . import _native
+        self._lib = _native.load()
+        self._native = _native
+        h = self._lib.fdtd_b200_batch_create(device)
+        if not h:
+            raise RuntimeError("fdtd_b200_batch_create failed: " + _native.last_error())
+        self._h = C.c_void_p(h)
+        self.members: list = []
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            self._lib.fdtd_b200_batch_destroy(self._h)
+            self._h = None
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what}: rc={rc} {self._native.last_error()}")
+
+    def set_segment(self, planes: int):
+        self._check(self._lib.fdtd_b200_batch_set_segment(self._h, int(planes)), "batch_set_segment")
+
+    def set(self, solvers, limits):
+        n = len(solvers)
+        arr = (C.c_void_p * max(n, 1))(*[s._h.value for s in solvers])
+        lim = np.ascontiguousarray(limits, dtype=np.int32)
+        self._check(self._lib.fdtd_b200_batch_set(self._h, C.cast(arr, C.POINTER(C.c_void_p)),
+                                                  lim.ctypes.data_as(C.POINTER(C.c_int)), n), "batch_set")
+        self.members = list(solvers)
+
+    def step(self, n_steps: int, use_graph: bool = True):
+        self._check(self._lib.fdtd_b200_batch_step(self._h, int(n_steps), 1 if use_graph else 0), "batch_step")
+
+    def sync(self):
+        n = max(len(self.members), 1)
+        steps = np.zeros(n, np.int32)
+        status = np.zeros(n, np.int32)
+        self._check(self._lib.fdtd_b200_batch_sync(self._h, steps.ctypes.data_as(C.POINTER(C.c_int)),
+                                                   status.ctypes.data_as(C.POINTER(C.c_int))), "batch_sync")
+        return steps[: len(self.members)], status[: len(self.members)]
+
+    @property
+    def launch_count(self) -> int:
+        return self._lib.fdtd_b200_batch_launch_count(self._h)
+
+
+# ---------------------------------------------------------------- schedulers
+class BatchServer:
+    """Continuous batching: admit on arrival when a slot and memory are free.
+
+    ``backend`` supplies ``make(room) -> solver``, ``batch() -> batch`` (with
+    set/step/sync) and ``traces(solver)``; the default uses the CUDA engine.
+    """
+
+    def __init__(self, max_slots: int = 64, mem_budget: Optional[int] = None, chunk: int = 64,
+                 use_graph: bool = True, seg_planes: int = 0, backend=None,
+                 clock: Callable[[], float] = time.perf_counter, sleep=time.sleep):
+        self.max_slots = max_slots
+        self.mem_budget = mem_budget
+        self.chunk = chunk
+        self.use_graph = use_graph
+        self.seg_planes = seg_planes
+        self.backend = backend or _EngineBackend()
+        self.clock = clock
+        self.sleep = sleep
+        self.log: List[dict] = []
+
+    def run(self, requests: Sequence[Request]) -> List[Result]:
+        be = self.backend
+        budget = self.mem_budget if self.mem_budget is not None else be.free_memory()
+        queue = deque(sorted(requests, key=lambda r: r.arrival))
+        batch = be.batch()
+        if self.seg_planes:
+            batch.set_segment(self.seg_planes)
+        active: List[tuple] = []          # (request, solver, start_time)
+        used = 0
+        results: List[Result] = []
+        t0 = self.clock()
+        dirty = False
+        while queue or active:
+            now = self.clock() - t0
+            while (queue and queue[0].arrival <= now and len(active) < self.max_slots
+                   and used + room_bytes(queue[0].room) <= budget):
+                req = queue.popleft()
+                active.append((req, be.make(req.room), now))
+                used += room_bytes(req.room)
+                dirty = True
+            if not active:
+                if queue and queue[0].arrival > now:
+                    self.sleep(min(queue[0].arrival - now, 0.05))
+                    continue
+                if queue:    # the next request does not fit even alone
+                    raise RuntimeError(f"request {queue[0].rid} exceeds the memory budget")
+                continue
+            if dirty:
+                batch.set([s for _, s, _ in active], [r.room.n_steps for r, _, _ in active])
+                dirty = False
+            batch.step(self.chunk, self.use_graph)
+            steps, status = batch.sync()
+            if np.any(status != 0):
+                bad = [active[q][0].rid for q in np.nonzero(status)[0]]
+                raise RuntimeError(f"requests {bad}: pressure diverged (FDTD_ERR_UNSTABLE)")
+            finished = [q for q, (r, _, _) in enumerate(active) if steps[q] >= r.room.n_steps]
+            self.log.append({"t": self.clock() - t0, "active": len(active), "finished": len(finished),
+                             "queued": len(queue)})
+            if finished:
+                keep = [a for q, a in enumerate(active) if q not in set(finished)]
+                done = [active[q] for q in finished]
+                batch.set([s for _, s, _ in keep], [r.room.n_steps for r, _, _ in keep])
+                t_done = self.clock() - t0
+                for req, solver, start in done:
+                    results.append(Result(req.rid, be.traces(solver), req.arrival, start, t_done))
+                    used -= room_bytes(req.room)
+                    be.release(solver)
+                active = keep
+                dirty = False
+        return sorted(results, key=lambda r: r.rid)
+
+
+class SequentialServer:
+    """Baseline: one request at a time through the plain single-room path."""
+
+    def __init__(self, backend=None, clock: Callable[[], float] = time.perf_counter, sleep=time.sleep):
+        self.backend = backend or _EngineBackend()
+        self.clock = clock
+        self.sleep = sleep
+
+    def run(self, requests: Sequence[Request]) -> List[Result]:
+        be = self.backend
+        results = []
+        t0 = self.clock()
+        for req in sorted(requests, key=lambda r: r.arrival):
+            now = self.clock() - t0
+            if req.arrival > now:
+                self.sleep(req.arrival - now)
+            start = self.clock() - t0
+            solver = be.make(req.room)
+            be.run_plain(solver, req.room.n_steps)
+            traces = be.traces(solver)
+            results.append(Result(req.rid, traces, req.arrival, start, self.clock() - t0))
+            be.release(solver)
+        return sorted(results, key=lambda r: r.rid)
+
+
+class _EngineBackend:
+    def __init__(self, device: Optional[int] = None):
+        import torch
+        self.device = torch.cuda.current_device() if device is None else device
+
+    def free_memory(self) -> int:
+        import torch
+        free, _ = torch.cuda.mem_get_info(self.device)
+        return int(free * 0.85)
+
+    def make(self, room: Room):
+        return make_solver(room, device=self.device)
+
+    def batch(self):
+        return EngineBatch(self.device)
+
+    def run_plain(self, solver, n_steps: int):
+        solver.step(n_steps)
+
+    def traces(self, solver) -> np.ndarray:
+        return solver.get_traces()
+
+    def release(self, solver):
+        solver.close()
+
+
+def calibrate_sequential(requests: Sequence[Request], backend=None) -> float:
+    """Mean plain-path service time (s) of the given requests run back to back."""
+    be = backend or _EngineBackend()
+    t0 = time.perf_counter()
+    for req in requests:
+        s = be.make(req.room)
+        be.run_plain(s, req.room.n_steps)
+        be.traces(s)
+        be.release(s)
+    return (time.perf_counter() - t0) / max(len(requests), 1)

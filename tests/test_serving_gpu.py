@@ -1,0 +1,112 @@
+"""Batched stepping on the GPU: each room is the same alone and in the mix."""
+import numpy as np
+import pytest
+
+from conftest import bits_equal, first_mismatch
+from spectral_analyzer_b200.rooms import seeded_room
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def cuda():
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.fail("a CUDA device is required for -m gpu tests")
+    return torch
+
+
+MIX = [(40, 36, 48, 150, 1), (64, 64, 64, 220, 2), (33, 90, 17, 95, 3), (100, 40, 130, 180, 4),
+       (16, 16, 16, 300, 5), (72, 48, 256, 120, 6)]
+
+
+def rooms():
+    out = []
+    for nx, ny, nz, steps, seed in MIX:
+        r = seeded_room(nx, ny, nz, steps, seed=seed, n_rec=3, n_pml=4,
+                        source_kind="gaussian" if seed % 2 else "ricker")
+        out.append(r)
+    return out
+
+
+def alone(room):
+    from spectral_analyzer_b200.serving import make_solver
+    f = make_solver(room)
+    f.set_kernel("fused")
+    f.step(room.n_steps)
+    return f.get_traces(), f.get_pressure_field(), f.get_velocity_z()
+
+
+@pytest.mark.parametrize("use_graph", [True, False])
+def test_batch_equals_alone(cuda, use_graph):
+    from spectral_analyzer_b200.serving import EngineBatch, make_solver
+    rs = rooms()
+    ref = [alone(r) for r in rs]
+    solvers = [make_solver(r) for r in rs]
+    b = EngineBatch()
+    b.set(solvers, [r.n_steps for r in rs])
+    steps = np.zeros(len(rs))
+    while np.any(steps < [r.n_steps for r in rs]):
+        b.step(37, use_graph)            # chunks that do not divide the step counts
+        steps, status = b.sync()
+        assert not status.any()
+    b.set([], [])
+    for r, f, (tr, P, Vz) in zip(rs, solvers, ref):
+        assert f.step_count == r.n_steps
+        got = f.get_traces()
+        assert bits_equal(got, tr), (r.describe(), first_mismatch(got, tr))
+        assert bits_equal(f.get_pressure_field(), P)
+        assert bits_equal(f.get_velocity_z(), Vz)
+
+
+def test_members_join_and_leave(cuda):
+    """Rooms enter mid-run and continue on the single-room path after leaving."""
+    from spectral_analyzer_b200.serving import EngineBatch, make_solver
+    rs = rooms()[:4]
+    ref = [alone(r) for r in rs]
+    s = [make_solver(r) for r in rs]
+    s[3].step(40)                        # some steps on the plain path first
+    b = EngineBatch()
+    b.set([s[0], s[1]], [rs[0].n_steps, rs[1].n_steps])
+    b.step(50)
+    b.sync()
+    b.set([s[0], s[1], s[2], s[3]], [r.n_steps for r in rs])     # 2 and 3 join
+    b.step(64)
+    b.sync()
+    b.set([s[1], s[2]], [rs[1].n_steps, rs[2].n_steps])          # 0 and 3 leave
+    s[0].step(rs[0].n_steps - s[0].step_count)                   # finish alone
+    s[3].step(rs[3].n_steps - s[3].step_count)
+    while s[1].step_count < rs[1].n_steps or s[2].step_count < rs[2].n_steps:
+        b.step(64)
+        b.sync()
+    b.set([], [])
+    for r, f, (tr, P, _) in zip(rs, s, ref):
+        assert f.step_count == r.n_steps
+        assert bits_equal(f.get_traces(), tr), r.describe()
+        assert bits_equal(f.get_pressure_field(), P)
+
+
+def test_batch_latches_instability(cuda):
+    from spectral_analyzer_b200.serving import EngineBatch, make_solver
+    rs = rooms()[:2]
+    s = [make_solver(r) for r in rs]
+    s[1].add_pressure(rs[1].src_flat, 1e9)
+    b = EngineBatch()
+    b.set(s, [300, 300])
+    b.step(300)
+    steps, status = b.sync()
+    assert list(steps) == [300, 300]
+    assert status[0] == 0 and status[1] == -3
+
+
+def test_batch_server_matches_sequential(cuda):
+    from spectral_analyzer_b200.serving import (BatchServer, SequentialServer, config3_requests,
+                                                poisson_arrivals)
+    reqs = config3_requests(10, seed=9, steps=(60, 260), axes=(32, 48, 64, 80))
+    for r, t in zip(reqs, poisson_arrivals(10, rate=400.0, seed=9)):
+        r.arrival = float(t)
+    seq = SequentialServer().run(reqs)
+    bat = BatchServer(max_slots=6, chunk=32).run(reqs)
+    for a, b in zip(seq, bat):
+        assert a.rid == b.rid
+        assert bits_equal(a.traces, b.traces), a.rid
