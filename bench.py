@@ -62,6 +62,10 @@ def parse_args():
                     help="NX,NY,NZ: a smaller seeded room of the same kind (profiling only)")
     ap.add_argument("--serve", action="store_true",
                     help="serving benchmark: continuous batching vs sequential plain launches")
+    ap.add_argument("--precision", action="store_true",
+                    help="storage-precision study (FP32/BF16/FP16, compensated) vs an FP64 GPU run")
+    ap.add_argument("--precision-steps", type=int, default=10000)
+    ap.add_argument("--precision-audit", type=int, default=500)
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-load", type=float, default=1.5,
                     help="offered load as a multiple of the sequential plain capacity")
@@ -390,14 +394,14 @@ def engine_arm(args):
 
 
 def serve_arm(args):
-    """Config-3 serving: Poisson arrivals at serve-load x the sequential capacity."""
+    """Serving 256 mixed rooms: Poisson arrivals at serve-load x the sequential capacity."""
     import torch
     from spectral_analyzer_b200 import autotune
     from spectral_analyzer_b200.serving import (BatchServer, SequentialServer, calibrate_sequential,
-                                                config3_requests, poisson_arrivals, request_work,
+                                                mixed_room_requests, poisson_arrivals, request_work,
                                                 summarize)
     torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-    reqs = config3_requests(args.serve_requests, seed=3, steps=(500, args.serve_max_steps))
+    reqs = mixed_room_requests(args.serve_requests, seed=3, steps=(500, args.serve_max_steps))
     tune = autotune.tune_segment()
     sample = reqs[:: max(1, len(reqs) // 16)]
     service = calibrate_sequential(sample)
@@ -412,7 +416,7 @@ def serve_arm(args):
     s_seq, s_bat = summarize(seq, work), summarize(bat, work)
     line = {"metric": "serve requests/s", "value": s_bat["requests_per_s"], "unit": "requests/s",
             "n_gpus": 1, "higher_is_better": True, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": "config3_rooms", "requests": len(reqs), "axes": "32..256 step 16",
+            "config": {"workload": "poisson_stream_rooms_32-256_cells_per_axis", "requests": len(reqs), "axes": "32..256 step 16",
                        "steps": [500, args.serve_max_steps], "receivers": "1..4",
                        "arrivals": "poisson", "offered_load_x_sequential": args.serve_load,
                        "arrival_rate_per_s": rate, "sequential_mean_service_s": service,
@@ -426,12 +430,41 @@ def serve_arm(args):
     return 0 if same else 1
 
 
+def precision_arm(args):
+    """Storage precision on the 512x384x256 room: traces and energy audit of each
+    storage mode against the FP64 GPU oracle run of the same room."""
+    import torch
+    from spectral_analyzer_b200.precision import study
+    from spectral_analyzer_b200.rooms import large_room, seeded_room
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    if GRID:
+        room = seeded_room(*GRID, args.precision_steps, seed=2, n_rec=8, source_kind="ricker")
+    else:
+        room = large_room(n_steps=args.precision_steps)
+    res = study(room, audit_every=args.precision_audit)
+    rows = {r["mode"]: r for r in res["modes"]}
+    line = {"metric": "receiver-trace rel L2 vs FP64 oracle", "value": rows["fp32"]["trace_rel_l2"],
+            "unit": "rel L2 (fp32 storage)", "n_gpus": 1, "higher_is_better": False,
+            "dtype": "f32 arithmetic; fp32/bf16/fp16 storage", "data": "synthetic",
+            "config": {"workload": f"room{room.nx}x{room.ny}x{room.nz}_ricker_storage_precision",
+                       "steps": room.n_steps, "receivers": len(room.receivers),
+                       "audit_every": args.precision_audit,
+                       "kernel": "two-pass, templated on storage (fdtd_precision.cu)"},
+            "fp64_oracle": {k: v for k, v in res["fp64"].items() if k != "energy"},
+            "energy_fp64": res["fp64"]["energy"],
+            "modes": rows}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
         return reference_arm(args)
     if args.serve:
         return serve_arm(args)
+    if args.precision:
+        return precision_arm(args)
     return engine_arm(args)
 
 

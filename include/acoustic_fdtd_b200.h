@@ -277,6 +277,44 @@ FDTD_B200_API int fdtd_b200_batch_step(FdtdB200Batch* b, int n_steps, int use_gr
 FDTD_B200_API int fdtd_b200_batch_sync(FdtdB200Batch* b, int* steps_out, int* status_out);
 FDTD_B200_API long long fdtd_b200_batch_launch_count(const FdtdB200Batch* b);
 
+/* ---- storage-precision study (no reference counterpart) ----
+ * An open room (no walls, fractions or plate; PML with per-face scales a6,
+ * NULL = all 1) stepped by the two-pass update with the fields stored as
+ *   mode 0 FP32, 1 FP64 (arithmetic in double: the GPU oracle),
+ *   2 BF16, 3 FP16, 4 BF16 + BF16 residual, 5 FP16 + FP16 residual;
+ * modes 2-5 compute in FP32 and round each stored value; the residual modes
+ * keep the FP32-formed remainder x - rn16(x) beside it (loads return the sum).
+ * FP16 fields are stored times p_scale (P) or v_scale (V), powers of two
+ * (<= 0 picks 2^10 and 2^19, right for source samples of order 1).
+ * Sources are deposited before a step, receivers (8 taps, summed in double)
+ * record after it, as fdtd_step + fdtd_sample_pressure_precomputed do. */
+typedef struct FdtdB200Prec FdtdB200Prec;
+FDTD_B200_API FdtdB200Prec* fdtd_b200_prec_create(int Nx, int Ny, int Nz, double dx, double c,
+                                                  double rho_air, int n_pml, const float* a6,
+                                                  int mode, float p_scale, float v_scale,
+                                                  int device);
+FDTD_B200_API void fdtd_b200_prec_destroy(FdtdB200Prec* p);
+FDTD_B200_API double fdtd_b200_prec_dt(const FdtdB200Prec* p);
+/* Source cell (flat reference index) and its per-step samples. */
+FDTD_B200_API int fdtd_b200_prec_set_source(FdtdB200Prec* p, int cell, const double* signal,
+                                            int n);
+/* Receivers as 8-tap samplers (fdtd_precompute_pressure_samplers layout),
+ * trace capacity in steps, and capacity of the energy-audit log. */
+FDTD_B200_API int fdtd_b200_prec_set_receivers(FdtdB200Prec* p, int n_rec, const int* idx8,
+                                               const double* wgt8, int capacity,
+                                               int audit_capacity);
+/* Launch n_steps steps; with audit_every > 0 the velocity pass of every step
+ * whose index is a multiple of it also sums the discrete energy in double. */
+FDTD_B200_API int fdtd_b200_prec_step(FdtdB200Prec* p, int n_steps, int audit_every);
+FDTD_B200_API int fdtd_b200_prec_get_traces(FdtdB200Prec* p, double* out, int out_len,
+                                            int* n_recorded);
+/* Rows (step n, potential part sum p^2/(rho c^2), energy E^n) with
+ * E^n = dx^3/2 (sum (p^n)^2/(rho c^2) + rho sum v^{n-1/2} v^{n+1/2}). */
+FDTD_B200_API int fdtd_b200_prec_get_energy(FdtdB200Prec* p, double* out3, int out_rows,
+                                            int* n_out);
+/* Current pressure, reference cell order, widened to double. */
+FDTD_B200_API int fdtd_b200_prec_get_pressure(FdtdB200Prec* p, double* out, int out_len);
+
 /* Number of kernels this handle has launched since creation. */
 FDTD_B200_API long long fdtd_b200_launch_count(const AcousticFDTDState* st);
 

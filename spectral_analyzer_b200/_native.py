@@ -17,6 +17,7 @@ i32 = C.c_int
 f32 = C.c_float
 P_i32 = C.POINTER(C.c_int)
 P_f32 = C.POINTER(C.c_float)
+P_f64 = C.POINTER(C.c_double)
 P_u8 = C.POINTER(C.c_uint8)
 
 # name -> (restype, argtypes); the 26 reference entry points first, then extensions
@@ -75,6 +76,16 @@ SIGNATURES = {
     "fdtd_b200_batch_step": (i32, [vp, i32, i32]),
     "fdtd_b200_batch_sync": (i32, [vp, P_i32, P_i32]),
     "fdtd_b200_batch_launch_count": (C.c_longlong, [vp]),
+    "fdtd_b200_prec_create": (vp, [i32, i32, i32, C.c_double, C.c_double, C.c_double, i32, P_f32,
+                                   i32, f32, f32, i32]),
+    "fdtd_b200_prec_destroy": (None, [vp]),
+    "fdtd_b200_prec_dt": (C.c_double, [vp]),
+    "fdtd_b200_prec_set_source": (i32, [vp, i32, P_f64, i32]),
+    "fdtd_b200_prec_set_receivers": (i32, [vp, i32, P_i32, P_f64, i32, i32]),
+    "fdtd_b200_prec_step": (i32, [vp, i32, i32]),
+    "fdtd_b200_prec_get_traces": (i32, [vp, P_f64, i32, P_i32]),
+    "fdtd_b200_prec_get_energy": (i32, [vp, P_f64, i32, P_i32]),
+    "fdtd_b200_prec_get_pressure": (i32, [vp, P_f64, i32]),
     "fdtd_b200_launch_count": (C.c_longlong, [vp]),
     "fdtd_b200_last_error": (C.c_char_p, []),
 }

@@ -35,8 +35,8 @@ def _load() -> Dict[str, dict]:
 
 
 def calibration_rooms(n: int = 12, seed: int = 21):
-    from .serving import config3_requests
-    return [r.room for r in config3_requests(n, seed=seed, steps=(200, 200))]
+    from .serving import mixed_room_requests
+    return [r.room for r in mixed_room_requests(n, seed=seed, steps=(200, 200))]
 
 
 def time_segment(rooms, planes: int, steps: int = 64, reps: int = 3) -> float:

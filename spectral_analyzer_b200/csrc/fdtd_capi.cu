@@ -32,6 +32,12 @@ void set_err(cudaError_t e, const char* what)
     snprintf(g_err, sizeof(g_err), "%s: %s (%d)", what, cudaGetErrorString(e), (int)e);
 }
 
+}  // namespace
+
+void fdtd::record_cuda_error(cudaError_t e, const char* what) { set_err(e, what); }
+
+namespace {
+
 #define CK(expr)                                   \
     do {                                           \
         cudaError_t e_ = (expr);                   \

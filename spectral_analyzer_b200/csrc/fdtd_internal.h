@@ -27,6 +27,9 @@ constexpr int kRowAlign = 8;           // floats per row-padding unit (32 B)
 constexpr int kCheckStride = 1013;     // stability sample stride (acoustic_fdtd.cpp:1250)
 constexpr int kCheckPeriod = 256;      // steps between checks (acoustic_fdtd.cpp:1284)
 
+// Records a CUDA error for fdtd_b200_last_error (defined in fdtd_capi.cu).
+void record_cuda_error(cudaError_t e, const char* what);
+
 struct Grid {
     int nx, ny, nz, sz;
     long long plane;   // ny * sz

@@ -55,7 +55,7 @@ def room_bytes(room: Room) -> int:
     return 8 * room.nx * room.ny * sz * 4 + room.n_steps * len(room.receivers) * 4 + (1 << 16)
 
 
-def config3_requests(n: int = 256, seed: int = 3, steps=(500, 8000), axes=GRID_AXES,
+def mixed_room_requests(n: int = 256, seed: int = 3, steps=(500, 8000), axes=GRID_AXES,
                      rec=(1, 4), a_range=(0.02, 0.3), n_pml: int = 10) -> List[Request]:
     """Rooms with axes drawn from ``axes``, steps U{steps}, 1-4 receivers, per-face
     absorption U[a_range], Gaussian or Ricker source, interior source/receivers."""

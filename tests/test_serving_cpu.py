@@ -2,7 +2,7 @@
 import numpy as np
 
 from spectral_analyzer_b200.rooms import Room
-from spectral_analyzer_b200.serving import (BatchServer, Request, SequentialServer, config3_requests,
+from spectral_analyzer_b200.serving import (BatchServer, Request, SequentialServer, mixed_room_requests,
                                             poisson_arrivals, room_bytes, summarize)
 
 
@@ -85,14 +85,14 @@ class FakeBackend:
 
 
 def small_requests(n=12, seed=1):
-    reqs = config3_requests(n, seed=seed, steps=(50, 400), axes=(32, 48, 64))
+    reqs = mixed_room_requests(n, seed=seed, steps=(50, 400), axes=(32, 48, 64))
     for r, t in zip(reqs, poisson_arrivals(n, rate=200.0, seed=seed)):
         r.arrival = float(t)
     return reqs
 
 
-def test_config3_generator_shapes():
-    reqs = config3_requests(256, seed=3)
+def test_mixed_room_generator_shapes():
+    reqs = mixed_room_requests(256, seed=3)
     assert len(reqs) == 256
     for r in reqs:
         rm = r.room
@@ -103,7 +103,7 @@ def test_config3_generator_shapes():
             assert all(0 <= c < d for c, d in zip(p, (rm.nx, rm.ny, rm.nz)))
     assert {r.room.source_kind for r in reqs} == {"gaussian", "ricker"}
     # seeded: the same list again
-    again = config3_requests(256, seed=3)
+    again = mixed_room_requests(256, seed=3)
     assert [r.room.describe() for r in reqs] == [r.room.describe() for r in again]
 
 

@@ -100,9 +100,9 @@ def test_batch_latches_instability(cuda):
 
 
 def test_batch_server_matches_sequential(cuda):
-    from spectral_analyzer_b200.serving import (BatchServer, SequentialServer, config3_requests,
+    from spectral_analyzer_b200.serving import (BatchServer, SequentialServer, mixed_room_requests,
                                                 poisson_arrivals)
-    reqs = config3_requests(10, seed=9, steps=(60, 260), axes=(32, 48, 64, 80))
+    reqs = mixed_room_requests(10, seed=9, steps=(60, 260), axes=(32, 48, 64, 80))
     for r, t in zip(reqs, poisson_arrivals(10, rate=400.0, seed=9)):
         r.arrival = float(t)
     seq = SequentialServer().run(reqs)
