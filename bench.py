@@ -66,6 +66,10 @@ def parse_args():
                     help="storage-precision study (FP32/BF16/FP16, compensated) vs an FP64 GPU run")
     ap.add_argument("--precision-steps", type=int, default=10000)
     ap.add_argument("--precision-audit", type=int, default=500)
+    ap.add_argument("--adjoint", action="store_true",
+                    help="gradient w.r.t. per-cell absorption: adjoint timing and checks")
+    ap.add_argument("--adjoint-steps", type=int, default=4000)
+    ap.add_argument("--adjoint-checkpoint", type=int, default=200)
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-load", type=float, default=1.5,
                     help="offered load as a multiple of the sequential plain capacity")
@@ -457,6 +461,91 @@ def precision_arm(args):
     return 0
 
 
+def adjoint_arm(args):
+    """Gradient of the 4-receiver trace loss w.r.t. per-cell boundary absorption on
+    the 128^3 room (4000 steps, checkpoints every 200): adjoint timing, central
+    finite differences on 16 seeded layer cells (double forward runs), and
+    torch.autograd on a 48^3 copy of the problem."""
+    import torch
+    from spectral_analyzer_b200.adjoint import AdjointRoom, differentiation_problem
+    from spectral_analyzer_b200.torch_reference import loss_and_grad
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    n = GRID[0] if GRID else 128
+    prob = differentiation_problem(n, n_steps=args.adjoint_steps, seed=5)
+    room = AdjointRoom(prob, checkpoint_every=args.adjoint_checkpoint)
+    room.set_absorption(prob.a_target)
+    tgt = room.forward(keep_checkpoints=False)
+    room.set_absorption(prob.a)
+    room.forward()                                  # warm-up of the checkpointed forward
+    g = room.backward(np.zeros((prob.n_steps, room.n_rec)))
+    l0 = room.launch_count
+    t0 = time.perf_counter()
+    y = room.forward()
+    t1 = time.perf_counter()
+    g = room.backward(2.0 * (y - tgt))
+    t2 = time.perf_counter()
+    launches = room.launch_count - l0
+    loss = float(np.sum((y - tgt) ** 2))
+    t_f, t_b = t1 - t0, t2 - t1
+    # central finite differences on 16 seeded layer cells, double forward runs
+    dbl = AdjointRoom(prob, double=True, checkpoint_every=args.adjoint_checkpoint)
+    a64 = prob.a.astype(np.float64)
+    rng = np.random.default_rng(16)
+    layer = np.argwhere(prob.a > 0)
+    cells = [tuple(int(v) for v in c) for c in layer[rng.choice(len(layer), 16, replace=False)]]
+    fd_rows = []
+    h = 1e-4
+    t3 = time.perf_counter()
+    for c in cells:
+        ap, am = a64.copy(), a64.copy()
+        ap[c] += h
+        am[c] -= h
+        fd = (dbl.loss(ap, tgt) - dbl.loss(am, tgt)) / (2 * h)
+        fd_rows.append({"cell": list(c), "adjoint": float(g[c]), "fd": fd,
+                        "rel_err": abs(float(g[c]) - fd) / abs(fd) if fd else None})
+    t_fd = time.perf_counter() - t3
+    fd_a = np.array([r["adjoint"] for r in fd_rows])
+    fd_v = np.array([r["fd"] for r in fd_rows])
+    dbl.close()
+    # torch.autograd on a 48^3 copy (float64), against the double and float adjoints
+    small = differentiation_problem(48, n_steps=args.adjoint_steps, seed=5)
+    out = {}
+    for name, double in (("double", True), ("float", False)):
+        r = AdjointRoom(small, double=double, checkpoint_every=args.adjoint_checkpoint)
+        r.set_absorption(small.a_target)
+        t_small = r.forward(keep_checkpoints=False)
+        if name == "double":
+            tgt_small = t_small
+        r.set_absorption(small.a)
+        ys = r.forward()
+        out[name] = r.backward(2.0 * (ys - tgt_small))
+        taps = r.taps
+        r.close()
+    t4 = time.perf_counter()
+    L_ref, g_ref = loss_and_grad(small.a, small, *taps, tgt_small, device="cuda")
+    t_torch = time.perf_counter() - t4
+    nrm = float(np.linalg.norm(g_ref))
+    line = {"metric": "adjoint gradient Gcell-steps/s (forward + backward)",
+            "value": prob.cells * prob.n_steps / (t_f + t_b) / 1e9, "unit": "Gcell-steps/s",
+            "n_gpus": 1, "higher_is_better": True, "dtype": "f32 (gradient accumulated in f64)",
+            "data": "synthetic",
+            "config": {"workload": f"room{n}^3_boundary_absorption_gradient", "steps": prob.n_steps,
+                       "receivers": len(prob.receivers), "checkpoint_every": args.adjoint_checkpoint,
+                       "absorption": "GRF corr 8 cells, clipped [0.05, 0.5], 10-cell layer",
+                       "targets": "float forward of the 10%-perturbed field"},
+            "loss": loss, "forward_s": t_f, "backward_s": t_b, "backward_over_forward": t_b / t_f,
+            "gpu_launches": launches,
+            "finite_differences": {"cells": 16, "h": h, "forward": "double", "seconds": t_fd,
+                                   "max_abs_err_over_max_abs_fd": float(np.max(np.abs(fd_a - fd_v)) / np.max(np.abs(fd_v))),
+                                   "median_rel_err": float(np.median(np.abs(fd_a - fd_v) / np.abs(fd_v))),
+                                   "rows": fd_rows},
+            "torch_autograd_48": {"loss": L_ref, "seconds": t_torch,
+                                  "double_adjoint_rel_l2": float(np.linalg.norm(out["double"] - g_ref)) / nrm,
+                                  "float_adjoint_rel_l2": float(np.linalg.norm(out["float"] - g_ref)) / nrm}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -465,6 +554,8 @@ def main():
         return serve_arm(args)
     if args.precision:
         return precision_arm(args)
+    if args.adjoint:
+        return adjoint_arm(args)
     return engine_arm(args)
 
 

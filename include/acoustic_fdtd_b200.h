@@ -315,6 +315,41 @@ FDTD_B200_API int fdtd_b200_prec_get_energy(FdtdB200Prec* p, double* out3, int o
 /* Current pressure, reference cell order, widened to double. */
 FDTD_B200_API int fdtd_b200_prec_get_pressure(FdtdB200Prec* p, double* out, int out_len);
 
+/* ---- gradient w.r.t. per-cell absorption (no reference counterpart) ----
+ * An open room whose absorption is a per-cell field a_c = alpha_c * dt in
+ * [0, 1] (the reference stores alpha per cell, acoustic_fdtd.cpp:64; here the
+ * whole field is an input): P damping 1/(1 + a_c), face damping
+ * 1 - (a_L + a_R)/2.  fdtd_b200_adj_forward runs n steps from rest (source
+ * deposited before each step, receivers recorded after it) and, with
+ * keep_checkpoints, stores p^n and v^{n-1/2} every checkpoint_every steps;
+ * fdtd_b200_adj_backward takes dL/dy (per step and receiver, the layout of
+ * the traces) and returns dL/da in reference cell order, recomputing the
+ * forward segment by segment and running the adjoint kernels backwards.
+ * use_double = 1 computes everything in double (for finite-difference checks);
+ * otherwise the arithmetic is float and the gradient accumulates in double.
+ * a_cell and grad_out may be host or device pointers. */
+typedef struct FdtdB200Adj FdtdB200Adj;
+FDTD_B200_API FdtdB200Adj* fdtd_b200_adj_create(int Nx, int Ny, int Nz, double dx, double c,
+                                                double rho_air, int use_double,
+                                                int checkpoint_every, int device);
+FDTD_B200_API void fdtd_b200_adj_destroy(FdtdB200Adj* h);
+FDTD_B200_API double fdtd_b200_adj_dt(const FdtdB200Adj* h);
+FDTD_B200_API long long fdtd_b200_adj_launch_count(const FdtdB200Adj* h);
+/* a_cell: Nx*Ny*Nz values of value_bytes (4 = float, 8 = double). */
+FDTD_B200_API int fdtd_b200_adj_set_absorption(FdtdB200Adj* h, const void* a_cell, int len,
+                                               int value_bytes);
+FDTD_B200_API int fdtd_b200_adj_set_source(FdtdB200Adj* h, int cell, const double* signal, int n);
+/* Receivers as 8-tap samplers; max_steps bounds the forward length. */
+FDTD_B200_API int fdtd_b200_adj_set_receivers(FdtdB200Adj* h, int n_rec, const int* idx8,
+                                              const double* wgt8, int max_steps);
+/* traces_out (host, may be NULL): n_steps x n_rec, widened to double. */
+FDTD_B200_API int fdtd_b200_adj_forward(FdtdB200Adj* h, int n_steps, int keep_checkpoints,
+                                        double* traces_out);
+/* dloss_dtrace (host): n_steps x n_rec of the last checkpointed forward;
+ * grad_out: Nx*Ny*Nz doubles. */
+FDTD_B200_API int fdtd_b200_adj_backward(FdtdB200Adj* h, const double* dloss_dtrace,
+                                         double* grad_out);
+
 /* Number of kernels this handle has launched since creation. */
 FDTD_B200_API long long fdtd_b200_launch_count(const AcousticFDTDState* st);
 

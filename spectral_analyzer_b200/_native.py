@@ -86,6 +86,15 @@ SIGNATURES = {
     "fdtd_b200_prec_get_traces": (i32, [vp, P_f64, i32, P_i32]),
     "fdtd_b200_prec_get_energy": (i32, [vp, P_f64, i32, P_i32]),
     "fdtd_b200_prec_get_pressure": (i32, [vp, P_f64, i32]),
+    "fdtd_b200_adj_create": (vp, [i32, i32, i32, C.c_double, C.c_double, C.c_double, i32, i32, i32]),
+    "fdtd_b200_adj_destroy": (None, [vp]),
+    "fdtd_b200_adj_dt": (C.c_double, [vp]),
+    "fdtd_b200_adj_launch_count": (C.c_longlong, [vp]),
+    "fdtd_b200_adj_set_absorption": (i32, [vp, vp, i32, i32]),
+    "fdtd_b200_adj_set_source": (i32, [vp, i32, P_f64, i32]),
+    "fdtd_b200_adj_set_receivers": (i32, [vp, i32, P_i32, P_f64, i32]),
+    "fdtd_b200_adj_forward": (i32, [vp, i32, i32, P_f64]),
+    "fdtd_b200_adj_backward": (i32, [vp, P_f64, vp]),
     "fdtd_b200_launch_count": (C.c_longlong, [vp]),
     "fdtd_b200_last_error": (C.c_char_p, []),
 }

@@ -1,0 +1,696 @@
+/*
+ * fdtd_adjoint.cu — gradient of a receiver-trace loss with respect to a
+ * per-cell absorption field, by the discrete adjoint of the open-room step.
+ *
+ * Forward (the reference's update with its PML profile replaced by a per-cell
+ * field a_c = alpha_c * dt, as csrc/kernels/acoustic_fdtd.cpp:64 and :387-389
+ * store alpha per cell; damping as :469-476 and :536-561):
+ *   p~^n       = p^n + s[n] e_src                                (source)
+ *   v^{n+1/2}  = (v^{n-1/2} - vc G p~^n) (.) d,  d_f = 1 - (a_L + a_R)/2
+ *   p^{n+1}    = (p~^n - bulk D v^{n+1/2}) (.) q,  q_c = 1 / (1 + a_c)
+ *   y^n        = R p^{n+1}                                       (receivers)
+ * with G the gradient (4th order on interior faces, 2nd order on the first
+ * and last face, acoustic_fdtd.cpp:1099-1148) and D the divergence (4th order
+ * with zero velocity outside the faces, :894-952).
+ *
+ * Reverse step n, given Lp = dL/dp~^{n+1} and Lv = dL/dv^{n+1/2} (partial,
+ * through step n+1's velocity update) and r^n = dL/dy^n:
+ *   lam  = Lp + R^T r^n                        (k_inject)
+ *   U    = lam (.) q ;  g_c -= q_c^2 lam_c z_c, z = p~^n - bulk D v^{n+1/2}   (k_adj_cells1)
+ *   mu   = Lv - bulk D^T U ;  W = mu (.) d ;  E_f = mu_f y_f,
+ *          y = v^{n-1/2} - vc G p~^n ;  Lv <- W                            (k_adj_faces)
+ *   Lp  <- U - vc G^T W ;  g_c -= 1/2 sum_{faces f of c} E_f               (k_adj_cells2)
+ * Gradients accumulate in double.  The forward is recomputed segment by
+ * segment from checkpoints (p^n and v^{n-1/2} every K steps) into K+1
+ * device slots, so the reverse sweep reads every state it needs from HBM.
+ *
+ * All kernels are templated on the working type R (float: the product path;
+ * double: for finite-difference checks).  Every operation is separately
+ * rounded (no contraction), so the float forward equals the reference's
+ * arithmetic on the same absorption field bit for bit.
+ */
+#include "acoustic_fdtd_b200.h"
+#include "fdtd_internal.h"
+
+#include <algorithm>
+#include <climits>
+#include <cstring>
+#include <vector>
+
+namespace fdtd {
+namespace adj {
+
+__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float rrcp(float a) { return __frcp_rn(a); }
+__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double rrcp(double a) { return __drcp_rn(a); }
+
+template <class R>
+struct ACoef {
+    R vc, bulk, c1, c2;
+};
+
+template <class R>
+__device__ __forceinline__ R face_d(R aL, R aR) { return rsub(R(1), rmul(R(0.5), radd(aL, aR))); }
+template <class R>
+__device__ __forceinline__ R cell_q(R a) { return rrcp(radd(R(1), a)); }
+
+// Gradient on face f = cell c's "+" face along an axis of n cells, at stride s.
+template <class R>
+__device__ __forceinline__ R grad_face(const R* p, long long id, long long s, int f, int n, const ACoef<R>& cf)
+{
+    const R pr = p[id + s], pc = p[id];
+    if (f > 0 && f < n - 2)
+        return radd(rmul(cf.c1, rsub(pr, pc)), rmul(cf.c2, rsub(p[id + 2 * s], p[id - s])));
+    return rsub(pr, pc);
+}
+
+// Divergence at cell c (index t along each axis), zero velocity outside faces.
+template <class R>
+__device__ __forceinline__ R div_cell(const Grid& g, const R* vx, const R* vy, const R* vz, long long id,
+                                      int i, int j, int k, const ACoef<R>& cf)
+{
+    const long long P = g.plane, S = g.sz;
+    const R z0 = R(0);
+    const R xp = (i < g.nx - 1) ? vx[id] : z0, xm = (i > 0) ? vx[id - P] : z0;
+    const R xpp = (i < g.nx - 2) ? vx[id + P] : z0, xmm = (i > 1) ? vx[id - 2 * P] : z0;
+    const R yp = (j < g.ny - 1) ? vy[id] : z0, ym = (j > 0) ? vy[id - S] : z0;
+    const R ypp = (j < g.ny - 2) ? vy[id + S] : z0, ymm = (j > 1) ? vy[id - 2 * S] : z0;
+    const R zp = (k < g.nz - 1) ? vz[id] : z0, zm = (k > 0) ? vz[id - 1] : z0;
+    const R zpp = (k < g.nz - 2) ? vz[id + 1] : z0, zmm = (k > 1) ? vz[id - 2] : z0;
+    const R d1 = radd(radd(rsub(xp, xm), rsub(yp, ym)), rsub(zp, zm));
+    const R d2 = radd(radd(rsub(xpp, xmm), rsub(ypp, ymm)), rsub(zpp, zmm));
+    return radd(rmul(cf.c1, d1), rmul(cf.c2, d2));
+}
+
+// Transposed divergence on face f of an axis with n cells, u at stride s.
+template <class R>
+__device__ __forceinline__ R divT_face(const R* u, long long id, long long s, int f, int n, const ACoef<R>& cf)
+{
+    R t = rmul(cf.c1, rsub(u[id], u[id + s]));
+    const R um = (f >= 1) ? u[id - s] : R(0);
+    const R upp = (f <= n - 3) ? u[id + 2 * s] : R(0);
+    return radd(t, rmul(cf.c2, rsub(um, upp)));
+}
+
+// Transposed gradient at cell t of an axis with n cells (faces 0..n-2), w at stride s.
+template <class R>
+__device__ __forceinline__ R gradT_cell(const R* w, long long id, long long s, int t, int n, const ACoef<R>& cf)
+{
+    R acc = R(0);
+    const int nf = n - 1;   // faces 0..n-2
+    auto inner = [&](int f) { return f > 0 && f < n - 2; };
+    if (t - 1 >= 0 && t - 1 < nf) acc = radd(acc, rmul(inner(t - 1) ? cf.c1 : R(1), w[id - s]));
+    if (t < nf) acc = rsub(acc, rmul(inner(t) ? cf.c1 : R(1), w[id]));
+    if (t - 2 >= 0 && inner(t - 2)) acc = radd(acc, rmul(cf.c2, w[id - 2 * s]));
+    if (t + 1 < nf && inner(t + 1)) acc = rsub(acc, rmul(cf.c2, w[id + s]));
+    return acc;
+}
+
+#define ADJ_INDEX                                                        \
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;                 \
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;                 \
+    const int i = blockIdx.z;                                            \
+    if (k >= g.nz || j >= g.ny) return;                                  \
+    const long long id = ((long long)i * g.ny + j) * g.sz + k;
+
+template <class R>
+__global__ void __launch_bounds__(256) k_fwd_vel(Grid g, ACoef<R> cf, const R* __restrict__ a,
+                                                 const R* __restrict__ p, const R* vin0, const R* vin1,
+                                                 const R* vin2, R* vout0, R* vout1, R* vout2)
+{
+    ADJ_INDEX
+    const R ac = a[id];
+    if (i < g.nx - 1)
+        vout0[id] = rmul(rsub(vin0[id], rmul(cf.vc, grad_face(p, id, g.plane, i, g.nx, cf))),
+                         face_d(ac, a[id + g.plane]));
+    if (j < g.ny - 1)
+        vout1[id] = rmul(rsub(vin1[id], rmul(cf.vc, grad_face(p, id, (long long)g.sz, j, g.ny, cf))),
+                         face_d(ac, a[id + g.sz]));
+    if (k < g.nz - 1)
+        vout2[id] = rmul(rsub(vin2[id], rmul(cf.vc, grad_face(p, id, 1LL, k, g.nz, cf))), face_d(ac, a[id + 1]));
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_fwd_pres(Grid g, ACoef<R> cf, const R* __restrict__ a,
+                                                  const R* __restrict__ p, const R* __restrict__ vx,
+                                                  const R* __restrict__ vy, const R* __restrict__ vz,
+                                                  R* __restrict__ pn)
+{
+    ADJ_INDEX
+    const R dv = div_cell(g, vx, vy, vz, id, i, j, k, cf);
+    pn[id] = rmul(rsub(p[id], rmul(cf.bulk, dv)), cell_q(a[id]));
+}
+
+// Source deposit into the (open) source cell before step n.
+template <class R>
+__global__ void k_deposit(R* p, long long src, const R* sig, int n)
+{
+    const R s = sig[n];
+    if (s != R(0)) p[src] = radd(p[src], s);
+}
+
+// Receivers after step n, summed as w0*p0 + w1*p1 + ... (acoustic_fdtd.cpp:1663-1676).
+template <class R>
+__global__ void k_record(const R* p, int n_rec, const long long* idx, const R* w, R* row)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= n_rec) return;
+    R s = rmul(w[8 * r], p[idx[8 * r]]);
+    for (int t = 1; t < 8; ++t) s = radd(s, rmul(w[8 * r + t], p[idx[8 * r + t]]));
+    row[r] = s;
+}
+
+// lam = Lp + R^T r^n: one thread, so taps that share a cell add in order.
+template <class R>
+__global__ void k_inject(R* lp, int n_rec, const long long* idx, const R* w, const R* rrow)
+{
+    for (int r = 0; r < n_rec; ++r)
+        for (int t = 0; t < 8; ++t) lp[idx[8 * r + t]] = radd(lp[idx[8 * r + t]], rmul(w[8 * r + t], rrow[r]));
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_adj_cells1(Grid g, ACoef<R> cf, const R* __restrict__ a,
+                                                    const R* __restrict__ lam, const R* __restrict__ pt,
+                                                    const R* __restrict__ vx, const R* __restrict__ vy,
+                                                    const R* __restrict__ vz, R* __restrict__ u,
+                                                    double* __restrict__ grad)
+{
+    ADJ_INDEX
+    const R q = cell_q(a[id]);
+    const R l = lam[id];
+    u[id] = rmul(l, q);
+    const R z = rsub(pt[id], rmul(cf.bulk, div_cell(g, vx, vy, vz, id, i, j, k, cf)));
+    grad[id] -= (double)q * (double)q * (double)l * (double)z;
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_adj_faces(Grid g, ACoef<R> cf, const R* __restrict__ a,
+                                                   const R* __restrict__ u, const R* __restrict__ pt,
+                                                   const R* __restrict__ vo0, const R* __restrict__ vo1,
+                                                   const R* __restrict__ vo2, R* lv0, R* lv1, R* lv2,
+                                                   R* __restrict__ e0, R* __restrict__ e1, R* __restrict__ e2)
+{
+    ADJ_INDEX
+    const R ac = a[id];
+    if (i < g.nx - 1) {
+        const R mu = rsub(lv0[id], rmul(cf.bulk, divT_face(u, id, g.plane, i, g.nx, cf)));
+        const R y = rsub(vo0[id], rmul(cf.vc, grad_face(pt, id, g.plane, i, g.nx, cf)));
+        lv0[id] = rmul(mu, face_d(ac, a[id + g.plane]));
+        e0[id] = rmul(mu, y);
+    }
+    if (j < g.ny - 1) {
+        const long long s = g.sz;
+        const R mu = rsub(lv1[id], rmul(cf.bulk, divT_face(u, id, s, j, g.ny, cf)));
+        const R y = rsub(vo1[id], rmul(cf.vc, grad_face(pt, id, s, j, g.ny, cf)));
+        lv1[id] = rmul(mu, face_d(ac, a[id + s]));
+        e1[id] = rmul(mu, y);
+    }
+    if (k < g.nz - 1) {
+        const R mu = rsub(lv2[id], rmul(cf.bulk, divT_face(u, id, 1LL, k, g.nz, cf)));
+        const R y = rsub(vo2[id], rmul(cf.vc, grad_face(pt, id, 1LL, k, g.nz, cf)));
+        lv2[id] = rmul(mu, face_d(ac, a[id + 1]));
+        e2[id] = rmul(mu, y);
+    }
+}
+
+template <class R>
+__global__ void __launch_bounds__(256) k_adj_cells2(Grid g, ACoef<R> cf, const R* __restrict__ u,
+                                                    const R* __restrict__ w0, const R* __restrict__ w1,
+                                                    const R* __restrict__ w2, const R* __restrict__ e0,
+                                                    const R* __restrict__ e1, const R* __restrict__ e2,
+                                                    R* __restrict__ lp, double* __restrict__ grad)
+{
+    ADJ_INDEX
+    const long long P = g.plane, S = g.sz;
+    R gt = gradT_cell(w0, id, P, i, g.nx, cf);
+    gt = radd(gt, gradT_cell(w1, id, S, j, g.ny, cf));
+    gt = radd(gt, gradT_cell(w2, id, 1LL, k, g.nz, cf));
+    lp[id] = rsub(u[id], rmul(cf.vc, gt));
+    double e = 0.0;
+    if (i < g.nx - 1) e += (double)e0[id];
+    if (i > 0) e += (double)e0[id - P];
+    if (j < g.ny - 1) e += (double)e1[id];
+    if (j > 0) e += (double)e1[id - S];
+    if (k < g.nz - 1) e += (double)e2[id];
+    if (k > 0) e += (double)e2[id - 1];
+    grad[id] -= 0.5 * e;
+}
+
+// a (reference order, float or double) -> padded R array
+template <class R, class T>
+__global__ void k_load_a(Grid g, const T* __restrict__ src, R* __restrict__ dst)
+{
+    ADJ_INDEX
+    dst[id] = (R)src[((long long)i * g.ny + j) * g.nz + k];
+}
+
+// padded double grad -> reference order (double)
+__global__ void k_store_grad(Grid g, const double* __restrict__ src, double* __restrict__ dst)
+{
+    ADJ_INDEX
+    dst[((long long)i * g.ny + j) * g.nz + k] = src[id];
+}
+
+}  // namespace adj
+}  // namespace fdtd
+
+using namespace fdtd;
+using namespace fdtd::adj;
+
+struct FdtdB200Adj {
+    int dbl = 0, device = 0, K = 200;
+    cudaStream_t stream = nullptr;
+    Grid g{};
+    int N = 0;
+    double dt = 0;
+    ACoef<float> c32{};
+    ACoef<double> c64{};
+    size_t eb = 4;                 // bytes per value of R
+    void* a = nullptr;             // padded R
+    // loss-mode state and checkpoints
+    void *P0 = nullptr, *P1 = nullptr, *V0[3] = {}, *V1[3] = {};
+    std::vector<void*> ckP, ckV;   // ckV holds 3 per checkpoint
+    // segment slots: K+1 P and K+1 x 3 V
+    std::vector<void*> sP, sV;
+    // adjoint state
+    void *Lp = nullptr, *U = nullptr, *Lv[3] = {}, *E[3] = {};
+    double* grad = nullptr;
+    double* grad_ref = nullptr;    // reference-order staging
+    // source/receivers
+    long long src = -1;
+    void* sig = nullptr;           // R[n_sig]
+    int n_sig = 0;
+    int n_rec = 0;
+    long long* ridx = nullptr;
+    void* rw = nullptr;            // R[8 n_rec]
+    void* traces = nullptr;        // R[n_steps x n_rec]
+    void* resid = nullptr;         // R[n_steps x n_rec]
+    int trace_cap = 0;
+    int fwd_steps = -1;            // steps of the last checkpointed forward
+    std::vector<void*> allocs;
+    long long launches = 0;
+};
+
+namespace {
+
+#define ACK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) { record_cuda_error(e_, #x); return FDTD_ERR_CUDA; } } while (0)
+
+int dalloc(FdtdB200Adj* h, void** p, size_t bytes)
+{
+    ACK(cudaMalloc(p, bytes));
+    h->allocs.push_back(*p);
+    ACK(cudaMemsetAsync(*p, 0, bytes, h->stream));
+    return FDTD_OK;
+}
+
+void dfree(FdtdB200Adj* h, void*& p)
+{
+    if (!p) return;
+    cudaFree(p);
+    h->allocs.erase(std::remove(h->allocs.begin(), h->allocs.end(), p), h->allocs.end());
+    p = nullptr;
+}
+
+size_t field_bytes(const FdtdB200Adj* h) { return (size_t)h->g.cells * h->eb; }
+
+dim3 cell_grid(const Grid& g) { return dim3((g.nz + 31) / 32, (g.ny + 7) / 8, g.nx); }
+const dim3 kBlock(32, 8, 1);
+
+template <class R>
+const ACoef<R>& coef(const FdtdB200Adj* h);
+template <>
+const ACoef<float>& coef<float>(const FdtdB200Adj* h) { return h->c32; }
+template <>
+const ACoef<double>& coef<double>(const FdtdB200Adj* h) { return h->c64; }
+
+// One forward step from (p, vin) to (pn, vout); p is first given the source.
+template <class R>
+void fwd_step(FdtdB200Adj* h, int n, void* p, void* const* vin, void* const* vout, void* pn)
+{
+    const Grid& g = h->g;
+    const ACoef<R>& cf = coef<R>(h);
+    if (h->src >= 0 && n < h->n_sig) {
+        k_deposit<R><<<1, 1, 0, h->stream>>>((R*)p, h->src, (const R*)h->sig, n);
+        ++h->launches;
+    }
+    k_fwd_vel<R><<<cell_grid(g), kBlock, 0, h->stream>>>(g, cf, (const R*)h->a, (const R*)p, (const R*)vin[0],
+                                                         (const R*)vin[1], (const R*)vin[2], (R*)vout[0],
+                                                         (R*)vout[1], (R*)vout[2]);
+    k_fwd_pres<R><<<cell_grid(g), kBlock, 0, h->stream>>>(g, cf, (const R*)h->a, (const R*)p, (const R*)vout[0],
+                                                          (const R*)vout[1], (const R*)vout[2], (R*)pn);
+    h->launches += 2;
+    if (h->n_rec > 0 && n < h->trace_cap) {
+        k_record<R><<<(h->n_rec + 31) / 32, 32, 0, h->stream>>>((const R*)pn, h->n_rec, h->ridx, (const R*)h->rw,
+                                                               (R*)h->traces + (size_t)n * h->n_rec);
+        ++h->launches;
+    }
+}
+
+template <class R>
+int forward_impl(FdtdB200Adj* h, int n_steps, int keep)
+{
+    const size_t fb = field_bytes(h);
+    ACK(cudaMemsetAsync(h->P0, 0, fb, h->stream));
+    for (int c = 0; c < 3; ++c) ACK(cudaMemsetAsync(h->V0[c], 0, fb, h->stream));
+    const int n_ck = keep ? (n_steps + h->K - 1) / h->K : 0;
+    while ((int)h->ckP.size() < n_ck) {
+        void* p = nullptr;
+        int rc = dalloc(h, &p, fb);
+        if (rc) return rc;
+        h->ckP.push_back(p);
+        for (int c = 0; c < 3; ++c) {
+            void* v = nullptr;
+            rc = dalloc(h, &v, fb);
+            if (rc) return rc;
+            h->ckV.push_back(v);
+        }
+    }
+    void* P[2] = {h->P0, h->P1};
+    void* V[2][3] = {{h->V0[0], h->V0[1], h->V0[2]}, {h->V1[0], h->V1[1], h->V1[2]}};
+    int cur = 0;
+    for (int n = 0; n < n_steps; ++n) {
+        if (keep && n % h->K == 0) {
+            const int q = n / h->K;
+            ACK(cudaMemcpyAsync(h->ckP[q], P[cur], fb, cudaMemcpyDeviceToDevice, h->stream));
+            for (int c = 0; c < 3; ++c)
+                ACK(cudaMemcpyAsync(h->ckV[3 * q + c], V[cur][c], fb, cudaMemcpyDeviceToDevice, h->stream));
+        }
+        fwd_step<R>(h, n, P[cur], V[cur], V[cur ^ 1], P[cur ^ 1]);
+        cur ^= 1;
+    }
+    ACK(cudaGetLastError());
+    h->fwd_steps = keep ? n_steps : -1;
+    return FDTD_OK;
+}
+
+int ensure_slots(FdtdB200Adj* h)
+{
+    const size_t fb = field_bytes(h);
+    while ((int)h->sP.size() < h->K + 1) {
+        void* p = nullptr;
+        int rc = dalloc(h, &p, fb);
+        if (rc) return rc;
+        h->sP.push_back(p);
+        for (int c = 0; c < 3; ++c) {
+            void* v = nullptr;
+            rc = dalloc(h, &v, fb);
+            if (rc) return rc;
+            h->sV.push_back(v);
+        }
+    }
+    if (!h->Lp) {
+        int rc = dalloc(h, &h->Lp, fb);
+        if (!rc) rc = dalloc(h, &h->U, fb);
+        for (int c = 0; c < 3 && !rc; ++c) rc = dalloc(h, &h->Lv[c], fb);
+        for (int c = 0; c < 3 && !rc; ++c) rc = dalloc(h, &h->E[c], fb);
+        if (!rc) {
+            void* gp = nullptr;
+            rc = dalloc(h, &gp, (size_t)h->g.cells * sizeof(double));
+            h->grad = (double*)gp;
+        }
+        if (!rc) {
+            void* gr = nullptr;
+            rc = dalloc(h, &gr, (size_t)h->N * sizeof(double));
+            h->grad_ref = (double*)gr;
+        }
+        if (rc) return rc;
+    }
+    return FDTD_OK;
+}
+
+template <class R>
+int backward_impl(FdtdB200Adj* h)
+{
+    const Grid& g = h->g;
+    const ACoef<R>& cf = coef<R>(h);
+    const size_t fb = field_bytes(h);
+    const int n_steps = h->fwd_steps;
+    ACK(cudaMemsetAsync(h->Lp, 0, fb, h->stream));
+    for (int c = 0; c < 3; ++c) {
+        ACK(cudaMemsetAsync(h->Lv[c], 0, fb, h->stream));
+        ACK(cudaMemsetAsync(h->E[c], 0, fb, h->stream));
+    }
+    ACK(cudaMemsetAsync(h->grad, 0, (size_t)g.cells * sizeof(double), h->stream));
+    const int n_seg = (n_steps + h->K - 1) / h->K;
+    for (int s = n_seg - 1; s >= 0; --s) {
+        const int n0 = s * h->K, n1 = std::min(n0 + h->K, n_steps), len = n1 - n0;
+        ACK(cudaMemcpyAsync(h->sP[0], h->ckP[s], fb, cudaMemcpyDeviceToDevice, h->stream));
+        for (int c = 0; c < 3; ++c)
+            ACK(cudaMemcpyAsync(h->sV[c], h->ckV[3 * s + c], fb, cudaMemcpyDeviceToDevice, h->stream));
+        // recompute: slot t holds p~^{n0+t} (after its deposit) and v^{n0+t-1/2}
+        const int saved_cap = h->trace_cap;
+        h->trace_cap = 0;   // traces are already recorded
+        for (int t = 0; t < len; ++t)
+            fwd_step<R>(h, n0 + t, h->sP[t], &h->sV[3 * t], &h->sV[3 * (t + 1)], h->sP[t + 1]);
+        h->trace_cap = saved_cap;
+        for (int t = len - 1; t >= 0; --t) {
+            const int n = n0 + t;
+            void* const* vo = &h->sV[3 * t];       // v^{n-1/2}
+            void* const* vn = &h->sV[3 * (t + 1)]; // v^{n+1/2}
+            if (h->n_rec > 0) {
+                k_inject<R><<<1, 1, 0, h->stream>>>((R*)h->Lp, h->n_rec, h->ridx, (const R*)h->rw,
+                                                    (const R*)h->resid + (size_t)n * h->n_rec);
+                ++h->launches;
+            }
+            k_adj_cells1<R><<<cell_grid(g), kBlock, 0, h->stream>>>(
+                g, cf, (const R*)h->a, (const R*)h->Lp, (const R*)h->sP[t], (const R*)vn[0], (const R*)vn[1],
+                (const R*)vn[2], (R*)h->U, h->grad);
+            k_adj_faces<R><<<cell_grid(g), kBlock, 0, h->stream>>>(
+                g, cf, (const R*)h->a, (const R*)h->U, (const R*)h->sP[t], (const R*)vo[0], (const R*)vo[1],
+                (const R*)vo[2], (R*)h->Lv[0], (R*)h->Lv[1], (R*)h->Lv[2], (R*)h->E[0], (R*)h->E[1],
+                (R*)h->E[2]);
+            k_adj_cells2<R><<<cell_grid(g), kBlock, 0, h->stream>>>(
+                g, cf, (const R*)h->U, (const R*)h->Lv[0], (const R*)h->Lv[1], (const R*)h->Lv[2],
+                (const R*)h->E[0], (const R*)h->E[1], (const R*)h->E[2], (R*)h->Lp, h->grad);
+            h->launches += 3;
+        }
+        ACK(cudaGetLastError());
+    }
+    return FDTD_OK;
+}
+
+template <class R>
+void set_coef(ACoef<R>& cf, R dx, R c, R rho, R dt)
+{
+    cf.vc = dt / (rho * dx);
+    const R inv_dx = R(1) / dx;
+    cf.bulk = rho * c * c * dt * inv_dx;
+    cf.c1 = R(9) / R(8);
+    cf.c2 = R(-1) / R(24);
+}
+
+long long pad_index(const Grid& g, int flat)
+{
+    const int k = flat % g.nz, t = flat / g.nz, j = t % g.ny, i = t / g.ny;
+    return ((long long)i * g.ny + j) * g.sz + k;
+}
+
+}  // namespace
+
+extern "C" {
+
+FdtdB200Adj* fdtd_b200_adj_create(int Nx, int Ny, int Nz, double dx, double c, double rho_air,
+                                  int use_double, int checkpoint_every, int device)
+{
+    if (Nx < 1 || Ny < 1 || Nz < 1 || dx <= 0 || c <= 0 || checkpoint_every < 1) return nullptr;
+    if ((long long)Nx * Ny * Nz > INT_MAX) return nullptr;
+    FdtdB200Adj* h = new FdtdB200Adj();
+    h->dbl = use_double ? 1 : 0;
+    h->eb = h->dbl ? 8 : 4;
+    h->K = checkpoint_every;
+    if (device < 0) cudaGetDevice(&device);
+    h->device = device;
+    if (cudaSetDevice(device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete h;
+        return nullptr;
+    }
+    Grid& g = h->g;
+    g.nx = Nx; g.ny = Ny; g.nz = Nz;
+    g.sz = (Nz + kRowAlign - 1) / kRowAlign * kRowAlign;
+    g.plane = (long long)Ny * g.sz;
+    g.cells = (long long)Nx * g.plane;
+    h->N = Nx * Ny * Nz;
+    // the reference's time step (acoustic_fdtd.cpp:345-349) in each working type
+    const float dt32 = 0.77f * (float)dx / ((float)c * 1.732050808f);
+    const double dt64 = 0.77 * dx / (c * 1.732050808);
+    set_coef<float>(h->c32, (float)dx, (float)c, (float)rho_air, dt32);
+    set_coef<double>(h->c64, dx, c, rho_air, dt64);
+    h->dt = h->dbl ? dt64 : (double)dt32;
+    const size_t fb = field_bytes(h);
+    int rc = dalloc(h, &h->a, fb);
+    if (!rc) rc = dalloc(h, &h->P0, fb);
+    if (!rc) rc = dalloc(h, &h->P1, fb);
+    for (int q = 0; q < 3 && !rc; ++q) rc = dalloc(h, &h->V0[q], fb);
+    for (int q = 0; q < 3 && !rc; ++q) rc = dalloc(h, &h->V1[q], fb);
+    if (!rc && cudaStreamSynchronize(h->stream) != cudaSuccess) rc = FDTD_ERR_CUDA;
+    if (rc) {
+        fdtd_b200_adj_destroy(h);
+        return nullptr;
+    }
+    return h;
+}
+
+void fdtd_b200_adj_destroy(FdtdB200Adj* h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void* p : h->allocs) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+double fdtd_b200_adj_dt(const FdtdB200Adj* h) { return h ? h->dt : 0.0; }
+
+long long fdtd_b200_adj_launch_count(const FdtdB200Adj* h) { return h ? h->launches : 0; }
+
+int fdtd_b200_adj_set_absorption(FdtdB200Adj* h, const void* a_cell, int len, int value_bytes)
+{
+    if (!h || !a_cell) return FDTD_ERR_NULL;
+    if (len != h->N) return FDTD_ERR_DIM;
+    if (value_bytes != 4 && value_bytes != 8) return FDTD_ERR_ARG;
+    ACK(cudaSetDevice(h->device));
+    void* stage = nullptr;
+    ACK(cudaMallocAsync(&stage, (size_t)len * value_bytes, h->stream));
+    cudaError_t e = cudaMemcpyAsync(stage, a_cell, (size_t)len * value_bytes, cudaMemcpyDefault, h->stream);
+    if (e == cudaSuccess) {
+        const Grid& g = h->g;
+        if (h->dbl && value_bytes == 8)
+            k_load_a<double, double><<<cell_grid(g), kBlock, 0, h->stream>>>(g, (const double*)stage, (double*)h->a);
+        else if (h->dbl)
+            k_load_a<double, float><<<cell_grid(g), kBlock, 0, h->stream>>>(g, (const float*)stage, (double*)h->a);
+        else if (value_bytes == 8)
+            k_load_a<float, double><<<cell_grid(g), kBlock, 0, h->stream>>>(g, (const double*)stage, (float*)h->a);
+        else
+            k_load_a<float, float><<<cell_grid(g), kBlock, 0, h->stream>>>(g, (const float*)stage, (float*)h->a);
+        e = cudaGetLastError();
+    }
+    cudaFreeAsync(stage, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+        record_cuda_error(e, "fdtd_b200_adj_set_absorption");
+        return FDTD_ERR_CUDA;
+    }
+    h->fwd_steps = -1;
+    return FDTD_OK;
+}
+
+int fdtd_b200_adj_set_source(FdtdB200Adj* h, int cell, const double* signal, int n)
+{
+    if (!h) return FDTD_ERR_NULL;
+    if (cell < 0 || cell >= h->N || n < 0 || (n > 0 && !signal)) return FDTD_ERR_ARG;
+    ACK(cudaSetDevice(h->device));
+    dfree(h, h->sig);
+    h->src = pad_index(h->g, cell);
+    h->n_sig = n;
+    if (n > 0) {
+        int rc = dalloc(h, &h->sig, (size_t)n * h->eb);
+        if (rc) return rc;
+        std::vector<unsigned char> buf((size_t)n * h->eb);
+        for (int q = 0; q < n; ++q) {
+            if (h->dbl) memcpy(&buf[(size_t)q * 8], &signal[q], 8);
+            else { const float f = (float)signal[q]; memcpy(&buf[(size_t)q * 4], &f, 4); }
+        }
+        ACK(cudaMemcpyAsync(h->sig, buf.data(), buf.size(), cudaMemcpyHostToDevice, h->stream));
+        ACK(cudaStreamSynchronize(h->stream));
+    }
+    h->fwd_steps = -1;
+    return FDTD_OK;
+}
+
+int fdtd_b200_adj_set_receivers(FdtdB200Adj* h, int n_rec, const int* idx8, const double* wgt8, int max_steps)
+{
+    if (!h || (n_rec > 0 && (!idx8 || !wgt8))) return FDTD_ERR_NULL;
+    if (n_rec < 0 || max_steps < 0) return FDTD_ERR_ARG;
+    std::vector<long long> pi((size_t)n_rec * 8);
+    for (size_t q = 0; q < pi.size(); ++q) {
+        if (idx8[q] < 0 || idx8[q] >= h->N) return FDTD_ERR_ARG;
+        pi[q] = pad_index(h->g, idx8[q]);
+    }
+    ACK(cudaSetDevice(h->device));
+    void* ri = h->ridx;
+    dfree(h, ri);
+    h->ridx = nullptr;
+    dfree(h, h->rw);
+    dfree(h, h->traces);
+    dfree(h, h->resid);
+    h->n_rec = n_rec;
+    h->trace_cap = max_steps;
+    if (n_rec > 0) {
+        void* p = nullptr;
+        int rc = dalloc(h, &p, pi.size() * sizeof(long long));
+        if (rc) return rc;
+        h->ridx = (long long*)p;
+        rc = dalloc(h, &h->rw, pi.size() * h->eb);
+        if (!rc) rc = dalloc(h, &h->traces, (size_t)std::max(max_steps, 1) * n_rec * h->eb);
+        if (!rc) rc = dalloc(h, &h->resid, (size_t)std::max(max_steps, 1) * n_rec * h->eb);
+        if (rc) return rc;
+        std::vector<unsigned char> wb(pi.size() * h->eb);
+        for (size_t q = 0; q < pi.size(); ++q) {
+            if (h->dbl) memcpy(&wb[q * 8], &wgt8[q], 8);
+            else { const float f = (float)wgt8[q]; memcpy(&wb[q * 4], &f, 4); }
+        }
+        ACK(cudaMemcpyAsync(h->ridx, pi.data(), pi.size() * sizeof(long long), cudaMemcpyHostToDevice, h->stream));
+        ACK(cudaMemcpyAsync(h->rw, wb.data(), wb.size(), cudaMemcpyHostToDevice, h->stream));
+        ACK(cudaStreamSynchronize(h->stream));
+    }
+    h->fwd_steps = -1;
+    return FDTD_OK;
+}
+
+int fdtd_b200_adj_forward(FdtdB200Adj* h, int n_steps, int keep_checkpoints, double* traces_out)
+{
+    if (!h) return FDTD_ERR_NULL;
+    if (n_steps < 1 || n_steps > h->trace_cap) return FDTD_ERR_DIM;
+    ACK(cudaSetDevice(h->device));
+    int rc = h->dbl ? forward_impl<double>(h, n_steps, keep_checkpoints)
+                    : forward_impl<float>(h, n_steps, keep_checkpoints);
+    if (rc) return rc;
+    if (traces_out && h->n_rec > 0) {
+        const size_t n = (size_t)n_steps * h->n_rec;
+        std::vector<unsigned char> buf(n * h->eb);
+        ACK(cudaMemcpyAsync(buf.data(), h->traces, buf.size(), cudaMemcpyDeviceToHost, h->stream));
+        ACK(cudaStreamSynchronize(h->stream));
+        for (size_t q = 0; q < n; ++q) {
+            if (h->dbl) memcpy(&traces_out[q], &buf[q * 8], 8);
+            else { float f; memcpy(&f, &buf[q * 4], 4); traces_out[q] = f; }
+        }
+    } else {
+        ACK(cudaStreamSynchronize(h->stream));
+    }
+    return FDTD_OK;
+}
+
+int fdtd_b200_adj_backward(FdtdB200Adj* h, const double* dloss_dtrace, double* grad_out)
+{
+    if (!h || !grad_out || (h->n_rec > 0 && !dloss_dtrace)) return FDTD_ERR_NULL;
+    if (h->fwd_steps < 1) return FDTD_ERR_ARG;    // needs a checkpointed forward of the current inputs
+    ACK(cudaSetDevice(h->device));
+    int rc = ensure_slots(h);
+    if (rc) return rc;
+    const size_t n = (size_t)h->fwd_steps * h->n_rec;
+    if (n > 0) {
+        std::vector<unsigned char> buf(n * h->eb);
+        for (size_t q = 0; q < n; ++q) {
+            if (h->dbl) memcpy(&buf[q * 8], &dloss_dtrace[q], 8);
+            else { const float f = (float)dloss_dtrace[q]; memcpy(&buf[q * 4], &f, 4); }
+        }
+        ACK(cudaMemcpyAsync(h->resid, buf.data(), buf.size(), cudaMemcpyHostToDevice, h->stream));
+        ACK(cudaStreamSynchronize(h->stream));
+    }
+    rc = h->dbl ? backward_impl<double>(h) : backward_impl<float>(h);
+    if (rc) return rc;
+    k_store_grad<<<cell_grid(h->g), kBlock, 0, h->stream>>>(h->g, h->grad, h->grad_ref);
+    ACK(cudaGetLastError());
+    ACK(cudaMemcpyAsync(grad_out, h->grad_ref, (size_t)h->N * sizeof(double), cudaMemcpyDefault, h->stream));
+    ACK(cudaStreamSynchronize(h->stream));
+    return FDTD_OK;
+}
+
+}  // extern "C"
