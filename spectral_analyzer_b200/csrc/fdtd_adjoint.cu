@@ -23,6 +23,9 @@
  * Gradients accumulate in double.  The forward is recomputed segment by
  * segment from checkpoints (p^n and v^{n-1/2} every K steps) into K+1
  * device slots, so the reverse sweep reads every state it needs from HBM.
+ * Each sweep (forward, forward with checkpoints, backward) is captured once
+ * as a CUDA graph and replayed while its length and buffers stay the same:
+ * a gradient evaluation is then two graph launches.
  *
  * All kernels are templated on the working type R (float: the product path;
  * double: for finite-difference checks).  Every operation is separately
@@ -294,6 +297,13 @@ struct FdtdB200Adj {
     int fwd_steps = -1;            // steps of the last checkpointed forward
     std::vector<void*> allocs;
     long long launches = 0;
+    // CUDA graphs of whole sweeps, replayed while the buffers they name live:
+    // forward without / with checkpoints (keyed by steps), backward (keyed by steps)
+    struct Sweep {
+        cudaGraphExec_t exec = nullptr;
+        int steps = -1;
+        long long launches = 0;
+    } fwd[2], bwd;
 };
 
 namespace {
@@ -351,13 +361,10 @@ void fwd_step(FdtdB200Adj* h, int n, void* p, void* const* vin, void* const* vou
     }
 }
 
-template <class R>
-int forward_impl(FdtdB200Adj* h, int n_steps, int keep)
+int ensure_checkpoints(FdtdB200Adj* h, int n_steps)
 {
     const size_t fb = field_bytes(h);
-    ACK(cudaMemsetAsync(h->P0, 0, fb, h->stream));
-    for (int c = 0; c < 3; ++c) ACK(cudaMemsetAsync(h->V0[c], 0, fb, h->stream));
-    const int n_ck = keep ? (n_steps + h->K - 1) / h->K : 0;
+    const int n_ck = (n_steps + h->K - 1) / h->K;
     while ((int)h->ckP.size() < n_ck) {
         void* p = nullptr;
         int rc = dalloc(h, &p, fb);
@@ -370,6 +377,16 @@ int forward_impl(FdtdB200Adj* h, int n_steps, int keep)
             h->ckV.push_back(v);
         }
     }
+    return FDTD_OK;
+}
+
+// The forward sweep (enqueued only; checkpoints must already exist).
+template <class R>
+int forward_impl(FdtdB200Adj* h, int n_steps, int keep)
+{
+    const size_t fb = field_bytes(h);
+    ACK(cudaMemsetAsync(h->P0, 0, fb, h->stream));
+    for (int c = 0; c < 3; ++c) ACK(cudaMemsetAsync(h->V0[c], 0, fb, h->stream));
     void* P[2] = {h->P0, h->P1};
     void* V[2][3] = {{h->V0[0], h->V0[1], h->V0[2]}, {h->V1[0], h->V1[1], h->V1[2]}};
     int cur = 0;
@@ -384,7 +401,48 @@ int forward_impl(FdtdB200Adj* h, int n_steps, int keep)
         cur ^= 1;
     }
     ACK(cudaGetLastError());
-    h->fwd_steps = keep ? n_steps : -1;
+    return FDTD_OK;
+}
+
+void drop_sweep(FdtdB200Adj::Sweep& g)
+{
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    g = FdtdB200Adj::Sweep();
+}
+
+void drop_sweeps(FdtdB200Adj* h)
+{
+    drop_sweep(h->fwd[0]);
+    drop_sweep(h->fwd[1]);
+    drop_sweep(h->bwd);
+}
+
+// Replays the cached graph of a sweep, capturing it first when it is missing
+// or was made for another length.  enqueue(h) issues the sweep on h->stream.
+template <class F>
+int run_sweep(FdtdB200Adj* h, FdtdB200Adj::Sweep& g, int steps, F enqueue)
+{
+    if (!g.exec || g.steps != steps) {
+        drop_sweep(g);
+        const long long l0 = h->launches;
+        ACK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = enqueue(h);
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(h->stream, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        ACK(e);
+        const cudaError_t ei = cudaGraphInstantiate(&g.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        ACK(ei);
+        g.steps = steps;
+        g.launches = h->launches - l0;
+        h->launches = l0;
+    }
+    ACK(cudaGraphLaunch(g.exec, h->stream));
+    h->launches += g.launches;
     return FDTD_OK;
 }
 
@@ -541,6 +599,7 @@ void fdtd_b200_adj_destroy(FdtdB200Adj* h)
     if (!h) return;
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
+    drop_sweeps(h);
     for (void* p : h->allocs) cudaFree(p);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
@@ -586,6 +645,8 @@ int fdtd_b200_adj_set_source(FdtdB200Adj* h, int cell, const double* signal, int
     if (!h) return FDTD_ERR_NULL;
     if (cell < 0 || cell >= h->N || n < 0 || (n > 0 && !signal)) return FDTD_ERR_ARG;
     ACK(cudaSetDevice(h->device));
+    ACK(cudaStreamSynchronize(h->stream));
+    drop_sweeps(h);
     dfree(h, h->sig);
     h->src = pad_index(h->g, cell);
     h->n_sig = n;
@@ -614,6 +675,8 @@ int fdtd_b200_adj_set_receivers(FdtdB200Adj* h, int n_rec, const int* idx8, cons
         pi[q] = pad_index(h->g, idx8[q]);
     }
     ACK(cudaSetDevice(h->device));
+    ACK(cudaStreamSynchronize(h->stream));
+    drop_sweeps(h);
     void* ri = h->ridx;
     dfree(h, ri);
     h->ridx = nullptr;
@@ -649,9 +712,14 @@ int fdtd_b200_adj_forward(FdtdB200Adj* h, int n_steps, int keep_checkpoints, dou
     if (!h) return FDTD_ERR_NULL;
     if (n_steps < 1 || n_steps > h->trace_cap) return FDTD_ERR_DIM;
     ACK(cudaSetDevice(h->device));
-    int rc = h->dbl ? forward_impl<double>(h, n_steps, keep_checkpoints)
-                    : forward_impl<float>(h, n_steps, keep_checkpoints);
+    const int keep = keep_checkpoints ? 1 : 0;
+    int rc = keep ? ensure_checkpoints(h, n_steps) : FDTD_OK;
     if (rc) return rc;
+    rc = run_sweep(h, h->fwd[keep], n_steps, [&](FdtdB200Adj* s) {
+        return s->dbl ? forward_impl<double>(s, n_steps, keep) : forward_impl<float>(s, n_steps, keep);
+    });
+    if (rc) return rc;
+    h->fwd_steps = keep ? n_steps : -1;
     if (traces_out && h->n_rec > 0) {
         const size_t n = (size_t)n_steps * h->n_rec;
         std::vector<unsigned char> buf(n * h->eb);
@@ -684,7 +752,9 @@ int fdtd_b200_adj_backward(FdtdB200Adj* h, const double* dloss_dtrace, double* g
         ACK(cudaMemcpyAsync(h->resid, buf.data(), buf.size(), cudaMemcpyHostToDevice, h->stream));
         ACK(cudaStreamSynchronize(h->stream));
     }
-    rc = h->dbl ? backward_impl<double>(h) : backward_impl<float>(h);
+    rc = run_sweep(h, h->bwd, h->fwd_steps, [](FdtdB200Adj* s) {
+        return s->dbl ? backward_impl<double>(s) : backward_impl<float>(s);
+    });
     if (rc) return rc;
     k_store_grad<<<cell_grid(h->g), kBlock, 0, h->stream>>>(h->g, h->grad, h->grad_ref);
     ACK(cudaGetLastError());
