@@ -70,6 +70,9 @@ def parse_args():
                     help="gradient w.r.t. per-cell absorption: adjoint timing and checks")
     ap.add_argument("--adjoint-steps", type=int, default=4000)
     ap.add_argument("--adjoint-checkpoint", type=int, default=200)
+    ap.add_argument("--decompose", action="store_true",
+                    help="split the room into slabs along i (torchrun ranks, or --slabs on one GPU)")
+    ap.add_argument("--slabs", type=int, default=2)
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-load", type=float, default=1.5,
                     help="offered load as a multiple of the sequential plain capacity")
@@ -546,6 +549,57 @@ def adjoint_arm(args):
     return 0
 
 
+def slab_arm(args):
+    """One room split along i: torchrun ranks exchange ghost planes over NCCL
+    (strong scaling of the same room); a single process steps --slabs slabs
+    on one GPU with plane-copy exchanges (checks the decomposition's cost)."""
+    import torch
+    import torch.distributed as dist
+    from spectral_analyzer_b200.slab import distributed_room, local_room
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    room = workload()
+    room.n_steps = args.steps + args.warmup
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+        run = distributed_room(room, rank, world)
+    else:
+        run = local_room(room, args.slabs)
+    run.step(args.warmup)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = sum(s.launch_count for s in run.slabs)
+    e0.record()
+    run.step(args.steps)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    launches = sum(s.launch_count for s in run.slabs) - l0
+    tr = run.traces(len(room.receivers))
+    ms_max = float(ms.item())
+    if rank == 0:
+        line = {"metric": METRIC, "value": room.cells * args.steps / (ms_max / 1e3) / 1e9,
+                "unit": "Gcell-updates/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "strong",
+                "dtype": "f32", "data": "synthetic",
+                "config": {"workload": room.name, "cells": room.cells,
+                           "parallelism": f"slab{world if world > 1 else args.slabs}",
+                           "exchange": "NCCL send/recv" if world > 1 else "in-process plane copies",
+                           "kernel": "two-pass slab kernels (fdtd_slab.cu)"},
+                "gpu_launches": launches, "traces_finite": bool(np.isfinite(tr).all())}
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -556,6 +610,8 @@ def main():
         return precision_arm(args)
     if args.adjoint:
         return adjoint_arm(args)
+    if args.decompose:
+        return slab_arm(args)
     return engine_arm(args)
 
 

@@ -350,6 +350,47 @@ FDTD_B200_API int fdtd_b200_adj_forward(FdtdB200Adj* h, int n_steps, int keep_ch
 FDTD_B200_API int fdtd_b200_adj_backward(FdtdB200Adj* h, const double* dloss_dtrace,
                                          double* grad_out);
 
+/* ---- one slab of a room split along i across GPUs (no reference counterpart) ----
+ * The slab owns global planes [i0, i1) (at least 2) of an open room and keeps
+ * two ghost planes each side: local plane l = global plane i0 - 2 + l,
+ * *local_planes = i1 - i0 + 4 planes of [Ny][Sz] floats per field.  The
+ * caller allocates five zeroed fields {P0, P1, Vx, Vy, Vz} of that size and
+ * exchanges ghosts between the passes: after fdtd_b200_slab_velocity the Vx
+ * planes 2,3 go to the left neighbour's planes own+2, own+3 and planes
+ * own, own+1 to the right neighbour's planes 0, 1; after
+ * fdtd_b200_slab_pressure the same for the current P (fdtd_b200_slab_current).
+ * One step: deposit(n), velocity, exchange Vx, pressure, exchange P, record.
+ * The source and receiver taps may lie in ghost planes (a source there is
+ * deposited into the ghost copy too); set them on every slab whose planes
+ * (ghosts included) hold them.  Kernels run on the stream of
+ * fdtd_b200_slab_set_stream (0 = the legacy default stream). */
+typedef struct FdtdB200Slab FdtdB200Slab;
+FDTD_B200_API int fdtd_b200_slab_layout(int Nx, int Ny, int Nz, int i0, int i1, int* local_planes,
+                                        int* sz);
+FDTD_B200_API FdtdB200Slab* fdtd_b200_slab_create(int Nx, int Ny, int Nz, int i0, int i1, float dx,
+                                                  float c, float rho_air, int n_pml,
+                                                  const float* a6, float* const* fields,
+                                                  int device);
+FDTD_B200_API void fdtd_b200_slab_destroy(FdtdB200Slab* h);
+FDTD_B200_API int fdtd_b200_slab_set_stream(FdtdB200Slab* h, void* stream);
+FDTD_B200_API float fdtd_b200_slab_dt(const FdtdB200Slab* h);
+/* Index (0 or 1) of the field holding the current pressure. */
+FDTD_B200_API int fdtd_b200_slab_current(const FdtdB200Slab* h);
+FDTD_B200_API long long fdtd_b200_slab_launch_count(const FdtdB200Slab* h);
+/* cell: global flat index; ignored (no source here) when outside this slab's planes. */
+FDTD_B200_API int fdtd_b200_slab_set_source(FdtdB200Slab* h, int cell, const float* signal, int n);
+/* Receivers as 8-tap samplers in global flat indices, every tap inside this slab's planes. */
+FDTD_B200_API int fdtd_b200_slab_set_receivers(FdtdB200Slab* h, int n_rec, const int* idx8,
+                                               const float* wgt8, int capacity);
+FDTD_B200_API int fdtd_b200_slab_deposit(FdtdB200Slab* h, int n);
+FDTD_B200_API int fdtd_b200_slab_velocity(FdtdB200Slab* h);
+FDTD_B200_API int fdtd_b200_slab_pressure(FdtdB200Slab* h);
+FDTD_B200_API int fdtd_b200_slab_record(FdtdB200Slab* h);
+/* Stability sample of the own cells (global flat phase + 1013 t); *bad = the
+ * smallest failing flat index or -1.  Synchronises the stream. */
+FDTD_B200_API int fdtd_b200_slab_check(FdtdB200Slab* h, int phase, long long* bad);
+FDTD_B200_API int fdtd_b200_slab_get_traces(FdtdB200Slab* h, float* out, int out_len, int* n_rows);
+
 /* Number of kernels this handle has launched since creation. */
 FDTD_B200_API long long fdtd_b200_launch_count(const AcousticFDTDState* st);
 

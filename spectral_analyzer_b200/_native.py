@@ -95,6 +95,21 @@ SIGNATURES = {
     "fdtd_b200_adj_set_receivers": (i32, [vp, i32, P_i32, P_f64, i32]),
     "fdtd_b200_adj_forward": (i32, [vp, i32, i32, P_f64]),
     "fdtd_b200_adj_backward": (i32, [vp, P_f64, vp]),
+    "fdtd_b200_slab_layout": (i32, [i32, i32, i32, i32, i32, P_i32, P_i32]),
+    "fdtd_b200_slab_create": (vp, [i32, i32, i32, i32, i32, f32, f32, f32, i32, P_f32, C.POINTER(vp), i32]),
+    "fdtd_b200_slab_destroy": (None, [vp]),
+    "fdtd_b200_slab_set_stream": (i32, [vp, vp]),
+    "fdtd_b200_slab_dt": (f32, [vp]),
+    "fdtd_b200_slab_current": (i32, [vp]),
+    "fdtd_b200_slab_launch_count": (C.c_longlong, [vp]),
+    "fdtd_b200_slab_set_source": (i32, [vp, i32, P_f32, i32]),
+    "fdtd_b200_slab_set_receivers": (i32, [vp, i32, P_i32, P_f32, i32]),
+    "fdtd_b200_slab_deposit": (i32, [vp, i32]),
+    "fdtd_b200_slab_velocity": (i32, [vp]),
+    "fdtd_b200_slab_pressure": (i32, [vp]),
+    "fdtd_b200_slab_record": (i32, [vp]),
+    "fdtd_b200_slab_check": (i32, [vp, i32, C.POINTER(C.c_longlong)]),
+    "fdtd_b200_slab_get_traces": (i32, [vp, P_f32, i32, P_i32]),
     "fdtd_b200_launch_count": (C.c_longlong, [vp]),
     "fdtd_b200_last_error": (C.c_char_p, []),
 }

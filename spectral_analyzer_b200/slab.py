@@ -1,0 +1,270 @@
+"""One room split along i over several ranks (one GPU each): slab decomposition.
+
+Rank r owns the planes ``partition(Nx, world)[r]`` and keeps two ghost planes
+on each side.  One step on every rank:
+
+    deposit(n)          source sample n into the local copy of the source cell
+                        (owned or ghost: the copies stay identical)
+    velocity()          own faces; reads P on the ghost planes
+    exchange("Vx")      2 planes of Vx to each neighbour
+    pressure()          own cells; reads Vx on the ghost planes
+    exchange("P")       2 planes of the new P to each neighbour
+    record()            receivers whose first tap lies in the own planes
+
+and every 256 steps the stability sample of the reference
+(csrc/kernels/acoustic_fdtd.cpp:1245-1268) over the own cells, reduced (min of
+the failing flat index) over ranks.  Each slab computes exactly what the
+whole-room kernels compute for its planes, so traces and fields equal the
+single-GPU engine's bit for bit.
+
+Backends: ``EngineSlab`` (the CUDA slab kernels, fields as torch CUDA
+tensors).  Exchanges: ``DistExchange`` (torch.distributed point-to-point:
+NCCL over NVLink between GPUs, or gloo between CPU processes) and
+``LocalExchange`` (several slabs in one process, plane copies).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import List, Sequence, Tuple
+
+import numpy as np
+
+from .precision import pressure_taps
+from .rooms import Room
+
+GHOST = 2
+CHECK_PERIOD, CHECK_STRIDE = 256, 1013
+
+
+def partition(nx: int, world: int) -> List[Tuple[int, int]]:
+    """Contiguous plane ranges, sizes differing by at most one, each >= 2 planes."""
+    if world < 1 or nx < 2 * world:
+        raise ValueError(f"cannot split {nx} planes over {world} ranks (2 planes per rank at least)")
+    base, rem = divmod(nx, world)
+    out, i = [], 0
+    for r in range(world):
+        n = base + (1 if r < rem else 0)
+        out.append((i, i + n))
+        i += n
+    return out
+
+
+def receiver_owner(room: Room, ranges: Sequence[Tuple[int, int]]) -> List[int]:
+    """Rank owning each receiver: the one whose planes hold its first tap."""
+    idx, _ = pressure_taps(room.nx, room.ny, room.nz, room.receiver_xyz())
+    planes = idx.reshape(-1, 8)[:, 0] // (room.ny * room.nz)
+    return [next(r for r, (a, b) in enumerate(ranges) if a <= p < b) for p in planes]
+
+
+class EngineSlab:
+    """CUDA backend: one fdtd_b200_slab handle over torch-allocated fields."""
+
+    def __init__(self, room: Room, i0: int, i1: int, rec_ids: Sequence[int], device=None):
+        import torch
+        from . import _native
+        self._native, self._lib = _native, _native.load()
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        L, sz = C.c_int(0), C.c_int(0)
+        rc = self._lib.fdtd_b200_slab_layout(room.nx, room.ny, room.nz, i0, i1, C.byref(L), C.byref(sz))
+        if rc != 0:
+            raise ValueError(f"slab [{i0}, {i1}) of {room.nx} planes: rc={rc}")
+        self.room, self.i0, self.i1, self.own = room, i0, i1, i1 - i0
+        self.L, self.sz = L.value, sz.value
+        self.fields = [torch.zeros((self.L, room.ny, self.sz), dtype=torch.float32, device=self.device)
+                       for _ in range(5)]
+        ptrs = (C.c_void_p * 5)(*[t.data_ptr() for t in self.fields])
+        a6 = np.ascontiguousarray(room.absorption, np.float32)
+        h = self._lib.fdtd_b200_slab_create(room.nx, room.ny, room.nz, i0, i1, room.dx, room.c, room.rho,
+                                            room.n_pml, a6.ctypes.data_as(_native.P_f32),
+                                            C.cast(ptrs, C.POINTER(C.c_void_p)), self.device.index)
+        if not h:
+            raise RuntimeError("fdtd_b200_slab_create failed: " + _native.last_error())
+        self._h = C.c_void_p(h)
+        self._check(self._lib.fdtd_b200_slab_set_stream(
+            self._h, C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)), "slab_set_stream")
+        sig = np.ascontiguousarray(room.signal(), np.float32)
+        self._check(self._lib.fdtd_b200_slab_set_source(self._h, room.src_flat,
+                                                        sig.ctypes.data_as(_native.P_f32), sig.size),
+                    "slab_set_source")
+        idx, w = pressure_taps(room.nx, room.ny, room.nz, room.receiver_xyz())
+        self.rec_ids = list(rec_ids)
+        sel = np.concatenate([np.arange(8 * r, 8 * r + 8) for r in self.rec_ids]) if self.rec_ids else \
+            np.zeros(0, np.int64)
+        self._idx = np.ascontiguousarray(idx[sel], np.int32)
+        self._w = np.ascontiguousarray(w[sel], np.float32)
+        self._check(self._lib.fdtd_b200_slab_set_receivers(
+            self._h, len(self.rec_ids), self._idx.ctypes.data_as(_native.P_i32),
+            self._w.ctypes.data_as(_native.P_f32), room.n_steps), "slab_set_receivers")
+
+    def _check(self, rc, what):
+        if rc != 0:
+            raise RuntimeError(f"{what}: rc={rc} {self._native.last_error()}")
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.fdtd_b200_slab_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def field(self, name: str):
+        if name == "P":
+            return self.fields[self._lib.fdtd_b200_slab_current(self._h)]
+        return self.fields[{"Vx": 2, "Vy": 3, "Vz": 4}[name]]
+
+    def deposit(self, n: int):
+        self._check(self._lib.fdtd_b200_slab_deposit(self._h, int(n)), "slab_deposit")
+
+    def velocity(self):
+        self._check(self._lib.fdtd_b200_slab_velocity(self._h), "slab_velocity")
+
+    def pressure(self):
+        self._check(self._lib.fdtd_b200_slab_pressure(self._h), "slab_pressure")
+
+    def record(self):
+        self._check(self._lib.fdtd_b200_slab_record(self._h), "slab_record")
+
+    def check(self, phase: int) -> int:
+        bad = C.c_longlong(0)
+        self._check(self._lib.fdtd_b200_slab_check(self._h, int(phase), C.byref(bad)), "slab_check")
+        return bad.value
+
+    def traces(self) -> np.ndarray:
+        n_rec = len(self.rec_ids)
+        out = np.empty(max(self.room.n_steps * n_rec, 1), np.float32)
+        rows = C.c_int(0)
+        self._check(self._lib.fdtd_b200_slab_get_traces(self._h, out.ctypes.data_as(self._native.P_f32),
+                                                        out.size, C.byref(rows)), "slab_get_traces")
+        return out[: rows.value * n_rec].reshape(rows.value, n_rec)
+
+    def own_pressure(self) -> np.ndarray:
+        """Current P of the own planes, (own, Ny, Nz)."""
+        p = self.field("P")[GHOST:GHOST + self.own, :, : self.room.nz]
+        return p.cpu().numpy()
+
+    @property
+    def launch_count(self) -> int:
+        return self._lib.fdtd_b200_slab_launch_count(self._h)
+
+
+class LocalExchange:
+    """Ghost exchange between slabs held by one process (ordered by i)."""
+
+    def __init__(self, slabs):
+        self.slabs = slabs
+
+    def exchange(self, name: str):
+        for a, b in zip(self.slabs[:-1], self.slabs[1:]):
+            fa, fb = a.field(name), b.field(name)
+            fb[0:GHOST].copy_(fa[a.own:a.own + GHOST])
+            fa[a.own + GHOST:a.own + 2 * GHOST].copy_(fb[GHOST:2 * GHOST])
+
+    def reduce_min(self, value: int) -> int:
+        return value
+
+    def gather(self, obj) -> list:
+        return [obj]
+
+
+class DistExchange:
+    """Ghost exchange with the neighbouring ranks over torch.distributed."""
+
+    def __init__(self, slab, rank: int, world: int, group=None):
+        self.slab, self.rank, self.world, self.group = slab, rank, world, group
+
+    def exchange(self, name: str):
+        import torch.distributed as dist
+        t, own = self.slab.field(name), self.slab.own
+        ops = []
+        if self.rank > 0:
+            ops += [dist.P2POp(dist.isend, t[GHOST:2 * GHOST], self.rank - 1, self.group),
+                    dist.P2POp(dist.irecv, t[0:GHOST], self.rank - 1, self.group)]
+        if self.rank < self.world - 1:
+            ops += [dist.P2POp(dist.isend, t[own:own + GHOST], self.rank + 1, self.group),
+                    dist.P2POp(dist.irecv, t[own + GHOST:own + 2 * GHOST], self.rank + 1, self.group)]
+        if ops:
+            for req in dist.batch_isend_irecv(ops):
+                req.wait()
+
+    def reduce_min(self, value: int) -> int:
+        import torch
+        import torch.distributed as dist
+        dev = self.slab.field("P").device
+        t = torch.tensor([value if value >= 0 else np.iinfo(np.int64).max], dtype=torch.int64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MIN, group=self.group)
+        v = int(t.item())
+        return -1 if v == np.iinfo(np.int64).max else v
+
+    def gather(self, obj) -> list:
+        import torch.distributed as dist
+        out = [None] * self.world
+        dist.all_gather_object(out, obj, group=self.group)
+        return out
+
+
+class SlabRunner:
+    """Steps the slabs of one room in lockstep with their ghost exchanges."""
+
+    def __init__(self, slabs, exchange):
+        self.slabs = list(slabs)
+        self.ex = exchange
+        self.step_count = 0
+        self.phase = 0
+
+    def step(self, n_steps: int = 1):
+        for _ in range(int(n_steps)):
+            for s in self.slabs:
+                s.deposit(self.step_count)
+            for s in self.slabs:
+                s.velocity()
+            self.ex.exchange("Vx")
+            for s in self.slabs:
+                s.pressure()
+            self.ex.exchange("P")
+            for s in self.slabs:
+                s.record()
+            self.step_count += 1
+            if self.step_count % CHECK_PERIOD == 0:
+                bads = [s.check(self.phase) for s in self.slabs]
+                bad = min([b for b in bads if b >= 0], default=-1)
+                bad = self.ex.reduce_min(bad)
+                self.phase = (self.phase + 1) % CHECK_STRIDE
+                if bad >= 0:
+                    raise RuntimeError("AcousticFDTD: pressure diverged (FDTD_ERR_UNSTABLE)")
+
+    def traces(self, n_rec: int) -> np.ndarray:
+        """All receivers' traces (steps, n_rec), assembled on every rank."""
+        parts = []
+        for s in self.slabs:
+            parts.append((list(s.rec_ids), s.traces()))
+        gathered = [p for obj in self.ex.gather(parts) for p in obj]
+        rows = max((t.shape[0] for _, t in gathered), default=0)
+        out = np.zeros((rows, n_rec), np.float32)
+        for ids, t in gathered:
+            for q, r in enumerate(ids):
+                out[:, r] = t[:, q]
+        return out
+
+    def pressure_field(self) -> np.ndarray:
+        """The whole room's current P (Nx, Ny, Nz), assembled on every rank."""
+        parts = [(s.i0, s.own_pressure()) for s in self.slabs]
+        gathered = sorted((p for obj in self.ex.gather(parts) for p in obj), key=lambda x: x[0])
+        return np.concatenate([p for _, p in gathered], axis=0)
+
+
+def local_room(room: Room, n_slabs: int, device=None) -> SlabRunner:
+    """All slabs of a room in this process on one GPU (tests, single-GPU runs)."""
+    ranges = partition(room.nx, n_slabs)
+    owners = receiver_owner(room, ranges)
+    slabs = [EngineSlab(room, a, b, [q for q, o in enumerate(owners) if o == r], device)
+             for r, (a, b) in enumerate(ranges)]
+    return SlabRunner(slabs, LocalExchange(slabs))
+
+
+def distributed_room(room: Room, rank: int, world: int, group=None, device=None) -> SlabRunner:
+    """This rank's slab of a room split over `world` ranks (torch.distributed initialised)."""
+    ranges = partition(room.nx, world)
+    owners = receiver_owner(room, ranges)
+    a, b = ranges[rank]
+    slab = EngineSlab(room, a, b, [q for q, o in enumerate(owners) if o == rank], device)
+    return SlabRunner([slab], DistExchange(slab, rank, world, group))
