@@ -142,57 +142,153 @@ __device__ __forceinline__ double block_sum(double v)
     return s;   // valid in thread (0,0)
 }
 
-// Velocity pass; with audit != nullptr also sum p^2 and v_old*v_new (double).
+// Four consecutive values (index i a multiple of 4, so the access is aligned:
+// rows start on 8-element boundaries).  Each value is decoded exactly as ld().
+template <int M>
+__device__ __forceinline__ void ld4(const Field& f, long long i, typename Traits<M>::A (&v)[4])
+{
+    using T = Traits<M>;
+    using S = typename T::S;
+    if constexpr (M == kFP32) {
+        const float4 x = *reinterpret_cast<const float4*>(static_cast<const float*>(f.hi) + i);
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    } else if constexpr (M == kFP64) {
+        const double2 x = *reinterpret_cast<const double2*>(static_cast<const double*>(f.hi) + i);
+        const double2 y = *reinterpret_cast<const double2*>(static_cast<const double*>(f.hi) + i + 2);
+        v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+    } else {
+        union { uint2 u; S s[4]; } h, l;
+        h.u = *reinterpret_cast<const uint2*>(static_cast<const S*>(f.hi) + i);
+        if constexpr (T::comp) l.u = *reinterpret_cast<const uint2*>(static_cast<const S*>(f.lo) + i);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            float x = tofl(h.s[q]);
+            if constexpr (T::comp) x = __fadd_rn(x, __fmul_rn(tofl(l.s[q]), f.inv_lo_scale));
+            v[q] = __fmul_rn(x, f.inv_scale);
+        }
+    }
+}
+
+// Four consecutive values, each encoded exactly as st().
+template <int M>
+__device__ __forceinline__ void st4(const Field& f, long long i, const typename Traits<M>::A (&v)[4])
+{
+    using T = Traits<M>;
+    using S = typename T::S;
+    if constexpr (M == kFP32) {
+        *reinterpret_cast<float4*>(static_cast<float*>(f.hi) + i) = make_float4(v[0], v[1], v[2], v[3]);
+    } else if constexpr (M == kFP64) {
+        *reinterpret_cast<double2*>(static_cast<double*>(f.hi) + i) = make_double2(v[0], v[1]);
+        *reinterpret_cast<double2*>(static_cast<double*>(f.hi) + i + 2) = make_double2(v[2], v[3]);
+    } else {
+        union { uint2 u; S s[4]; } h, l;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const float xs = __fmul_rn(v[q], f.scale);
+            h.s[q] = fromfl<S>(xs);
+            if constexpr (T::comp) l.s[q] = fromfl<S>(__fmul_rn(__fsub_rn(xs, tofl(h.s[q])), f.lo_scale));
+        }
+        *reinterpret_cast<uint2*>(static_cast<S*>(f.hi) + i) = h.u;
+        if constexpr (T::comp) *reinterpret_cast<uint2*>(static_cast<S*>(f.lo) + i) = l.u;
+    }
+}
+
+#define PREC_INDEX                                                        \
+    const int k0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);           \
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;                  \
+    const int i = blockIdx.z;                                             \
+    const bool live = k0 < g.nz && j < g.ny;                              \
+    const long long id = ((long long)i * g.ny + j) * g.sz + k0;
+
+// Velocity pass over four cells per thread (k0 .. k0+3); with audit !=
+// nullptr it also sums p^2 and v_old*v_new (double).  Faces that do not exist
+// (and row padding) keep their stored zero.
 template <int M>
 __global__ void __launch_bounds__(256) k_vel(Grid g, PCoef<typename Traits<M>::A> cf, Field p,
                                              Field vx, Field vy, Field vz, double* audit)
 {
     using A = typename Traits<M>::A;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
+    PREC_INDEX
     double e_p = 0.0, e_v = 0.0;
-    if (k < g.nz && j < g.ny) {
-        const long long id = ((long long)i * g.ny + j) * g.sz + k;
-        const A ay = cf.ay[j], az = cf.az[k];
-        const A ac = amax(amax(cf.ax[i], ay), az);
-        const A pc = ld<M>(p, id);
-        if (audit) e_p = (double)pc * (double)pc;
+    if (live) {
+        A pc[4], az4[4], ac[4];
+        ld4<M>(p, id, pc);
+        const A ay = cf.ay[j], axi = cf.ax[i];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = k0 + q;
+            az4[q] = k < g.nz ? cf.az[k] : A(0);
+            ac[q] = amax(amax(axi, ay), az4[q]);
+            if (audit && k < g.nz) e_p += (double)pc[q] * (double)pc[q];
+        }
+        // x faces
         if (i < g.nx - 1) {
-            const A pr = ld<M>(p, id + g.plane);
-            A grad;
-            if (i > 0 && i < g.nx - 2)
-                grad = radd(rmul(cf.c1, rsub(pr, pc)), rmul(cf.c2, rsub(ld<M>(p, id + 2 * g.plane), ld<M>(p, id - g.plane))));
-            else
-                grad = rsub(pr, pc);
-            const A vo = ld<M>(vx, id);
-            const A v = rmul(rsub(vo, rmul(cf.vc, grad)), fdamp(ac, amax(amax(cf.ax[i + 1], ay), az), cf.dt));
-            st<M>(vx, id, v);
-            if (audit) e_v += (double)vo * (double)v;
+            const bool fourth = i > 0 && i < g.nx - 2;
+            A pr[4], pm[4], p2[4], vo[4], vn[4];
+            ld4<M>(p, id + g.plane, pr);
+            if (fourth) {
+                ld4<M>(p, id - g.plane, pm);
+                ld4<M>(p, id + 2 * g.plane, p2);
+            }
+            ld4<M>(vx, id, vo);
+            const A axr = cf.ax[i + 1];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                vn[q] = vo[q];
+                if (k0 + q < g.nz) {
+                    const A grad = fourth ? radd(rmul(cf.c1, rsub(pr[q], pc[q])), rmul(cf.c2, rsub(p2[q], pm[q])))
+                                          : rsub(pr[q], pc[q]);
+                    vn[q] = rmul(rsub(vo[q], rmul(cf.vc, grad)), fdamp(ac[q], amax(amax(axr, ay), az4[q]), cf.dt));
+                    if (audit) e_v += (double)vo[q] * (double)vn[q];
+                }
+            }
+            st4<M>(vx, id, vn);
         }
+        // y faces
         if (j < g.ny - 1) {
-            const A pr = ld<M>(p, id + g.sz);
-            A grad;
-            if (j > 0 && j < g.ny - 2)
-                grad = radd(rmul(cf.c1, rsub(pr, pc)), rmul(cf.c2, rsub(ld<M>(p, id + 2 * g.sz), ld<M>(p, id - g.sz))));
-            else
-                grad = rsub(pr, pc);
-            const A vo = ld<M>(vy, id);
-            const A v = rmul(rsub(vo, rmul(cf.vc, grad)), fdamp(ac, amax(amax(cf.ax[i], cf.ay[j + 1]), az), cf.dt));
-            st<M>(vy, id, v);
-            if (audit) e_v += (double)vo * (double)v;
+            const bool fourth = j > 0 && j < g.ny - 2;
+            A pr[4], pm[4], p2[4], vo[4], vn[4];
+            ld4<M>(p, id + g.sz, pr);
+            if (fourth) {
+                ld4<M>(p, id - g.sz, pm);
+                ld4<M>(p, id + 2 * g.sz, p2);
+            }
+            ld4<M>(vy, id, vo);
+            const A ayr = cf.ay[j + 1];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                vn[q] = vo[q];
+                if (k0 + q < g.nz) {
+                    const A grad = fourth ? radd(rmul(cf.c1, rsub(pr[q], pc[q])), rmul(cf.c2, rsub(p2[q], pm[q])))
+                                          : rsub(pr[q], pc[q]);
+                    vn[q] = rmul(rsub(vo[q], rmul(cf.vc, grad)), fdamp(ac[q], amax(amax(axi, ayr), az4[q]), cf.dt));
+                    if (audit) e_v += (double)vo[q] * (double)vn[q];
+                }
+            }
+            st4<M>(vy, id, vn);
         }
-        if (k < g.nz - 1) {
-            const A pr = ld<M>(p, id + 1);
-            A grad;
-            if (k > 0 && k < g.nz - 2)
-                grad = radd(rmul(cf.c1, rsub(pr, pc)), rmul(cf.c2, rsub(ld<M>(p, id + 2), ld<M>(p, id - 1))));
-            else
-                grad = rsub(pr, pc);
-            const A vo = ld<M>(vz, id);
-            const A v = rmul(rsub(vo, rmul(cf.vc, grad)), fdamp(ac, amax(amax(cf.ax[i], ay), cf.az[k + 1]), cf.dt));
-            st<M>(vz, id, v);
-            if (audit) e_v += (double)vo * (double)v;
+        // z faces: P at k0-1 .. k0+5 (ext[t] = P[k0 - 1 + t])
+        {
+            A ext[7], vo[4], vn[4];
+            ext[0] = k0 > 0 ? ld<M>(p, id - 1) : A(0);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) ext[q + 1] = pc[q];
+            ext[5] = k0 + 4 < g.nz ? ld<M>(p, id + 4) : A(0);
+            ext[6] = k0 + 5 < g.nz ? ld<M>(p, id + 5) : A(0);
+            ld4<M>(vz, id, vo);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int k = k0 + q;
+                vn[q] = vo[q];
+                if (k < g.nz - 1) {
+                    const A grad = (k > 0 && k < g.nz - 2)
+                                       ? radd(rmul(cf.c1, rsub(ext[q + 2], ext[q + 1])), rmul(cf.c2, rsub(ext[q + 3], ext[q])))
+                                       : rsub(ext[q + 2], ext[q + 1]);
+                    vn[q] = rmul(rsub(vo[q], rmul(cf.vc, grad)), fdamp(ac[q], amax(amax(axi, ay), cf.az[k + 1]), cf.dt));
+                    if (audit) e_v += (double)vo[q] * (double)vn[q];
+                }
+            }
+            st4<M>(vz, id, vn);
         }
     }
     if (audit) {   // uniform per launch
@@ -206,35 +302,51 @@ __global__ void __launch_bounds__(256) k_vel(Grid g, PCoef<typename Traits<M>::A
     }
 }
 
+// Pressure pass over four cells per thread.
 template <int M>
 __global__ void __launch_bounds__(256) k_pres(Grid g, PCoef<typename Traits<M>::A> cf, Field p, Field pn,
                                               Field vx, Field vy, Field vz)
 {
     using A = typename Traits<M>::A;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k >= g.nz || j >= g.ny) return;
-    const long long id = ((long long)i * g.ny + j) * g.sz + k;
+    PREC_INDEX
+    if (!live) return;
     const long long P = g.plane, S = g.sz;
+    A xp[4] = {}, xm[4] = {}, xpp[4] = {}, xmm[4] = {}, yp[4] = {}, ym[4] = {}, ypp[4] = {}, ymm[4] = {};
+    if (i < g.nx - 1) ld4<M>(vx, id, xp);
+    if (i > 0) ld4<M>(vx, id - P, xm);
+    if (i < g.nx - 2) ld4<M>(vx, id + P, xpp);
+    if (i > 1) ld4<M>(vx, id - 2 * P, xmm);
+    if (j < g.ny - 1) ld4<M>(vy, id, yp);
+    if (j > 0) ld4<M>(vy, id - S, ym);
+    if (j < g.ny - 2) ld4<M>(vy, id + S, ypp);
+    if (j > 1) ld4<M>(vy, id - 2 * S, ymm);
+    // Vz at k0-2 .. k0+4: ext[t] = Vz[k0 - 2 + t]
+    A ext[7], vzc[4], pc[4], out[4];
+    ld4<M>(vz, id, vzc);
+    ext[0] = k0 >= 2 ? ld<M>(vz, id - 2) : A(0);
+    ext[1] = k0 >= 1 ? ld<M>(vz, id - 1) : A(0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ext[q + 2] = vzc[q];
+    ext[6] = k0 + 4 < g.nz ? ld<M>(vz, id + 4) : A(0);
+    ld4<M>(p, id, pc);
     const A z0 = A(0);
-    const A xp = (i < g.nx - 1) ? ld<M>(vx, id) : z0;
-    const A xm = (i > 0) ? ld<M>(vx, id - P) : z0;
-    const A xpp = (i < g.nx - 2) ? ld<M>(vx, id + P) : z0;
-    const A xmm = (i > 1) ? ld<M>(vx, id - 2 * P) : z0;
-    const A yp = (j < g.ny - 1) ? ld<M>(vy, id) : z0;
-    const A ym = (j > 0) ? ld<M>(vy, id - S) : z0;
-    const A ypp = (j < g.ny - 2) ? ld<M>(vy, id + S) : z0;
-    const A ymm = (j > 1) ? ld<M>(vy, id - 2 * S) : z0;
-    const A zp = (k < g.nz - 1) ? ld<M>(vz, id) : z0;
-    const A zm = (k > 0) ? ld<M>(vz, id - 1) : z0;
-    const A zpp = (k < g.nz - 2) ? ld<M>(vz, id + 1) : z0;
-    const A zmm = (k > 1) ? ld<M>(vz, id - 2) : z0;
-    const A d1 = radd(radd(rsub(xp, xm), rsub(yp, ym)), rsub(zp, zm));
-    const A d2 = radd(radd(rsub(xpp, xmm), rsub(ypp, ymm)), rsub(zpp, zmm));
-    const A dv = radd(rmul(cf.c1, d1), rmul(cf.c2, d2));
-    const A pd = amin(amin(cf.px[i], cf.py[j]), cf.pz[k]);
-    st<M>(pn, id, rmul(rsub(ld<M>(p, id), rmul(cf.bulk, dv)), pd));
+    const A pxy = amin(cf.px[i], cf.py[j]);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int k = k0 + q;
+        out[q] = z0;
+        if (k < g.nz) {
+            const A zp = (k < g.nz - 1) ? ext[q + 2] : z0;
+            const A zm = (k > 0) ? ext[q + 1] : z0;
+            const A zpp = (k < g.nz - 2) ? ext[q + 3] : z0;
+            const A zmm = (k > 1) ? ext[q] : z0;
+            const A d1 = radd(radd(rsub(xp[q], xm[q]), rsub(yp[q], ym[q])), rsub(zp, zm));
+            const A d2 = radd(radd(rsub(xpp[q], xmm[q]), rsub(ypp[q], ymm[q])), rsub(zpp, zmm));
+            const A dv = radd(rmul(cf.c1, d1), rmul(cf.c2, d2));
+            out[q] = rmul(rsub(pc[q], rmul(cf.bulk, dv)), amin(pxy, cf.pz[k]));
+        }
+    }
+    st4<M>(pn, id, out);
 }
 
 // Source deposit into an open cell (the rooms here have no solid cells) and
@@ -366,7 +478,7 @@ int step_impl(FdtdB200Prec* p, int n, int audit_every)
     using A = typename Traits<M>::A;
     const PCoef<A>& cf = *reinterpret_cast<const PCoef<A>*>(M == kFP64 ? (const void*)&p->cf64 : (const void*)&p->cf32);
     const Grid& g = p->g;
-    dim3 block(32, 8, 1), grid((g.nz + 31) / 32, (g.ny + 7) / 8, g.nx);
+    dim3 block(32, 8, 1), grid((g.sz / 4 + 31) / 32, (g.ny + 7) / 8, g.nx);
     for (int s = 0; s < n; ++s) {
         Field& P = p->f[p->cur];
         Field& PN = p->f[p->cur ^ 1];
