@@ -591,7 +591,8 @@ def slab_arm(args):
                 "config": {"workload": room.name, "cells": room.cells,
                            "parallelism": f"slab{world if world > 1 else args.slabs}",
                            "exchange": "NCCL send/recv" if world > 1 else "in-process plane copies",
-                           "kernel": "two-pass slab kernels (fdtd_slab.cu)"},
+                           "kernel": ("fused single-pass kernel on slabs, one exchange per step" if run.fused
+                                      else "two-pass slab kernels, two exchanges per step")},
                 "gpu_launches": launches, "traces_finite": bool(np.isfinite(tr).all())}
         print(json.dumps(line), flush=True)
     if world > 1:

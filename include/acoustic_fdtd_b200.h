@@ -351,15 +351,18 @@ FDTD_B200_API int fdtd_b200_adj_backward(FdtdB200Adj* h, const double* dloss_dtr
                                          double* grad_out);
 
 /* ---- one slab of a room split along i across GPUs (no reference counterpart) ----
- * The slab owns global planes [i0, i1) (at least 2) of an open room and keeps
- * two ghost planes each side: local plane l = global plane i0 - 2 + l,
- * *local_planes = i1 - i0 + 4 planes of [Ny][Sz] floats per field.  The
- * caller allocates five zeroed fields {P0, P1, Vx, Vy, Vz} of that size and
- * exchanges ghosts between the passes: after fdtd_b200_slab_velocity the Vx
- * planes 2,3 go to the left neighbour's planes own+2, own+3 and planes
- * own, own+1 to the right neighbour's planes 0, 1; after
- * fdtd_b200_slab_pressure the same for the current P (fdtd_b200_slab_current).
- * One step: deposit(n), velocity, exchange Vx, pressure, exchange P, record.
+ * The slab owns global planes [i0, i1) (at least 3) of an open room and keeps
+ * three ghost planes each side: local plane l = global plane i0 - 3 + l,
+ * *local_planes = i1 - i0 + 6 planes of [Ny][Sz] floats per field.  The
+ * caller allocates eight zeroed fields {P0, P1, Vx0, Vy0, Vz0, Vx1, Vy1, Vz1}
+ * of that size (two pressure buffers, two velocity sets) and exchanges ghost
+ * planes with the neighbours: P of the current buffer (fdtd_b200_slab_current)
+ * planes 3,4,5 to the left neighbour's own+3 .. own+5 and own .. own+2 to the
+ * right neighbour's 0 .. 2; Vx of the current set (fdtd_b200_slab_vset)
+ * planes 3,4 to the left neighbour's own+3, own+4 and own+1, own+2 to the
+ * right neighbour's 1, 2.
+ * Fused step: deposit(n), step, exchange P and Vx, record.
+ * Two-pass step: deposit(n), velocity, exchange Vx, pressure, exchange P, record.
  * The source and receiver taps may lie in ghost planes (a source there is
  * deposited into the ghost copy too); set them on every slab whose planes
  * (ghosts included) hold them.  Kernels run on the stream of
@@ -374,8 +377,9 @@ FDTD_B200_API FdtdB200Slab* fdtd_b200_slab_create(int Nx, int Ny, int Nz, int i0
 FDTD_B200_API void fdtd_b200_slab_destroy(FdtdB200Slab* h);
 FDTD_B200_API int fdtd_b200_slab_set_stream(FdtdB200Slab* h, void* stream);
 FDTD_B200_API float fdtd_b200_slab_dt(const FdtdB200Slab* h);
-/* Index (0 or 1) of the field holding the current pressure. */
+/* Index (0 or 1) of the field holding the current pressure / velocity set. */
 FDTD_B200_API int fdtd_b200_slab_current(const FdtdB200Slab* h);
+FDTD_B200_API int fdtd_b200_slab_vset(const FdtdB200Slab* h);
 FDTD_B200_API long long fdtd_b200_slab_launch_count(const FdtdB200Slab* h);
 /* cell: global flat index; ignored (no source here) when outside this slab's planes. */
 FDTD_B200_API int fdtd_b200_slab_set_source(FdtdB200Slab* h, int cell, const float* signal, int n);
@@ -383,6 +387,8 @@ FDTD_B200_API int fdtd_b200_slab_set_source(FdtdB200Slab* h, int cell, const flo
 FDTD_B200_API int fdtd_b200_slab_set_receivers(FdtdB200Slab* h, int n_rec, const int* idx8,
                                                const float* wgt8, int capacity);
 FDTD_B200_API int fdtd_b200_slab_deposit(FdtdB200Slab* h, int n);
+/* Fused single-pass step of the own planes (flips both current indices). */
+FDTD_B200_API int fdtd_b200_slab_step(FdtdB200Slab* h);
 FDTD_B200_API int fdtd_b200_slab_velocity(FdtdB200Slab* h);
 FDTD_B200_API int fdtd_b200_slab_pressure(FdtdB200Slab* h);
 FDTD_B200_API int fdtd_b200_slab_record(FdtdB200Slab* h);

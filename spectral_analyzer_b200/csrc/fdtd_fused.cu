@@ -266,9 +266,13 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int tk = tile % tiles_k, tj = tile / tiles_k;
     const int j0 = tj * C::TJ, k0 = tk * C::TK;
-    const int i_beg = seg * seg_len;
-    if (i_beg >= nx) return true;
-    const int i_end = min(i_beg + seg_len, nx);
+    // own planes and the global frame (a slab of a split room, or the whole room)
+    const bool slab = a.xs.nxg > 0;
+    const int nxg = slab ? a.xs.nxg : nx, xg0 = slab ? a.xs.xg0 : 0;
+    const int own_lo = slab ? a.xs.i_lo : 0, own_hi = slab ? a.xs.i_lo + a.xs.n_own : nx;
+    const int i_beg = own_lo + seg * seg_len;
+    if (i_beg >= own_hi) return true;
+    const int i_end = min(i_beg + seg_len, own_hi);
     const Coef cf = a.cf;
 
     __syncthreads();   // the previous tile's readers of the tables are done
@@ -290,8 +294,8 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
         const unsigned pb = bar0 + 8u * ps;
         mbar_expect_tx(pb, C::P_BYTES);
         tma_load3(sbase + 4u * (C::RING0 + ps * C::P_STAGE), tmP, k0 - 4, j0 - 3, u, pb);
-        const int f = u - 2, io = u - 3;
-        const bool vx = (u >= i_beg && f >= 0 && f <= nx - 2);
+        const int f = u - 2, io = u - 3, fg = f + xg0;
+        const bool vx = (u >= i_beg && fg >= 0 && fg <= nxg - 2);
         const bool vyz = (io >= i_beg && io < i_end);
         const unsigned vb = bar0 + 8u * (C::RING + vsg);
         const unsigned vdst = sbase + 4u * (C::VST0 + vsg * C::V_STAGE);
@@ -390,10 +394,10 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
 
         // ---- new Vx on face f = u-2 of the own columns (planes f-1 .. f+2) ----
         if (u >= i_beg) {
-            const int f = u - 2;
+            const int f = u - 2, fg = f + xg0;
             float4 vnew = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (f >= 0 && f <= nx - 2 && row_ok) {
-                const bool fourth = (f > 0 && f < nx - 2);
+            if (fg >= 0 && fg <= nxg - 2 && row_ok) {
+                const bool fourth = (fg > 0 && fg < nxg - 2);
                 const float axf = axw2, axf1 = axw1;     // alpha_x[f], alpha_x[f+1]
                 const float4 pm = lds4(smem + C::RING0 + pslot[0] * C::P_STAGE + cP);
                 const float4 p0 = lds4(smem + C::RING0 + pslot[1] * C::P_STAGE + cP);
@@ -586,7 +590,7 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
                                                       const __grid_constant__ CUtensorMap tmZ,
                                                       int seg_len, int tiles_k)
 {
-    if ((int)blockIdx.y * seg_len >= a.g.nx) return;
+    if ((int)blockIdx.y * seg_len >= (a.xs.nxg > 0 ? a.xs.n_own : a.g.nx)) return;
     float* smem;
     const unsigned sbase = smem_base_u32<C>(&smem);
     const unsigned bar0 = sbase + 4u * C::BAR0;
@@ -639,6 +643,7 @@ __global__ void __launch_bounds__(C::NT, 2) k_fused_batch(BatchMember* __restric
             a.vout[c] = m->v[par ^ 1][c];
         }
         a.status = status;
+        a.xs = XSpan{0, 0, 0, 0};
         const int local = item - m->items_begin;
         if (!fused_tile<C>(a, &m->maps[par][0], &m->maps[par][1], &m->maps[par][2], &m->maps[par][3],
                            local % m->tiles, local / m->tiles, m->seg_len, m->tiles_k, smem, sbase,
@@ -790,11 +795,12 @@ cudaError_t launch_fused_step(const FusedArgs& a, FusedCache* cache, cudaStream_
     // segments along i: as many as one wave of resident CTAs holds (every CTA
     // marches the same number of planes, so a single full wave has no tail)
     const long long slots = (long long)g_slots_per_sm[dev] * g_sms[dev];
+    const int n_own = a.xs.nxg > 0 ? a.xs.n_own : g.nx;
     long long segs = slots / tiles;
     if (segs < 1) segs = 1;
-    if (segs > g.nx) segs = g.nx;
-    const int seg_len = (int)((g.nx + segs - 1) / segs);
-    segs = (g.nx + seg_len - 1) / seg_len;
+    if (segs > n_own) segs = n_own;
+    const int seg_len = (int)((n_own + segs - 1) / segs);
+    segs = (n_own + seg_len - 1) / seg_len;
     dim3 grid((unsigned)tiles, (unsigned)segs, 1);
     k_fused_step<C><<<grid, C::NT, C::SMEM_BYTES, s>>>(a, maps[0], maps[1], maps[2], maps[3], seg_len,
                                                        tiles_k);

@@ -130,15 +130,27 @@ cudaError_t launch_check(const Grid& g, const float* p, long long n_cells, int p
                          unsigned* status, int step, cudaStream_t s);
 
 // ---- fused single-pass step (fdtd_fused.cu) ----
+// A slab of a room split along i: the local grid holds planes of the global
+// room from xg0 on and the step computes the local planes [i_lo, i_lo+n_own);
+// face existence and gradient order follow the global index.  nxg = 0 means
+// the local grid is the whole room (all planes own).
+struct XSpan {
+    int xg0;     // global index of local plane 0
+    int nxg;     // global Nx, or 0
+    int i_lo;    // first own local plane
+    int n_own;   // own planes
+};
+
 struct FusedArgs {
     Grid g;
     Coef cf;
-    Tables tb;
+    Tables tb;             // tb.ax / tb.px per local plane
     const float* p;        // P^n
     float* pn;             // P^{n+1}
     const float* vin[3];   // V^{n-1/2}: Vx, Vy, Vz
     float* vout[3];        // V^{n+1/2}
     unsigned* status;      // kStatusTimeout is set if a load wait runs out
+    XSpan xs;              // zero: whole room
 };
 struct FusedCache;         // host-side TMA descriptors of a handle's fields
 FusedCache* fused_cache_create();

@@ -2,18 +2,23 @@
  * fdtd_slab.cu — one slab of a room split along i across GPUs.
  *
  * A rank owns the planes [i0, i1) of an open room (no walls, fractions or
- * plate) and stores them with two ghost planes on each side: local plane l
- * is global plane x0 + l, x0 = i0 - 2, L = i1 - i0 + 4 planes of the usual
- * [plane][Ny][Sz] layout.  The step is the two-pass update of
- * fdtd_general.cu with every boundary decision taken on the global index,
- * so a slab computes exactly what the whole-room kernels compute for its
- * planes, provided its ghosts hold the neighbours' values:
- *   velocity of the own faces needs P on local planes 1 .. own+3,
- *   pressure of the own cells needs Vx on local planes 0 .. own+2.
- * The host exchanges the ghost planes between the passes (two planes of Vx
- * after the velocity pass, two planes of P after the pressure pass, per
- * neighbour, acoustic_fdtd.cpp:1108-1109 and :935-938 are the stencils that
- * need them).  A source in a ghost plane is deposited into the ghost copy as
+ * plate) and stores them with three ghost planes on each side: local plane l
+ * is global plane x0 + l, x0 = i0 - 3, L = i1 - i0 + 6 planes of the usual
+ * [plane][Ny][Sz] layout.  Every boundary decision is taken on the global
+ * index, so a slab computes exactly what the whole-room kernels compute for
+ * its planes, provided its ghosts hold the neighbours' values.  Two steps:
+ *   fused (fdtd_b200_slab_step): the single-pass TMA kernel of
+ *     fdtd_fused.cu on the own planes; it recomputes the new Vx of the two
+ *     faces left and one face right of the slab from ghost P (local planes
+ *     0 .. own+5) and ghost old Vx (local faces 1 .. own+3), so one exchange
+ *     per step suffices: 3 planes of the new P and 2 of the new Vx per
+ *     neighbour after the step;
+ *   two-pass (fdtd_b200_slab_velocity, then _pressure): velocity of the own
+ *     faces needs P on local planes 2 .. own+4, pressure of the own cells
+ *     needs Vx on local planes 1 .. own+3; Vx is exchanged between the passes
+ *     and P after them.
+ * (acoustic_fdtd.cpp:1108-1109 and :935-938 are the stencils that need the
+ * ghosts.)  A source in a ghost plane is deposited into the ghost copy as
  * well, so the copies stay identical without another exchange.
  *
  * Kernels run on the stream set with fdtd_b200_slab_set_stream (the caller's
@@ -32,7 +37,7 @@ struct Slab {
     Grid g;        // local grid: nx = L planes
     int x0;        // global index of local plane 0
     int nxg;       // global Nx
-    int own_lo;    // first own local plane (2)
+    int own_lo;    // first own local plane (3)
 };
 
 __device__ __forceinline__ float slab_alpha(const Tables& tb, int l, float ay, float az)
@@ -170,8 +175,9 @@ struct FdtdB200Slab {
     Tables tb{};
     float* d_tab = nullptr;
     float* P[2] = {};
-    float* V[3] = {};
-    int cur = 0;
+    float* V[2][3] = {};
+    int cur = 0, cv = 0;
+    FusedCache* fcache = nullptr;
     long long src = -1;
     float* d_sig = nullptr;
     int n_sig = 0;
@@ -181,6 +187,7 @@ struct FdtdB200Slab {
     float* d_trace = nullptr;
     int cap = 0, rows = 0;
     unsigned long long* d_bad = nullptr;
+    unsigned* d_status = nullptr;   // timeout word of the fused step
     long long launches = 0;
 };
 
@@ -209,8 +216,8 @@ extern "C" {
 
 int fdtd_b200_slab_layout(int Nx, int Ny, int Nz, int i0, int i1, int* local_planes, int* sz)
 {
-    if (Nx < 1 || Ny < 1 || Nz < 1 || i0 < 0 || i1 > Nx || i1 - i0 < 2) return FDTD_ERR_DIM;
-    if (local_planes) *local_planes = i1 - i0 + 4;
+    if (Nx < 1 || Ny < 1 || Nz < 1 || i0 < 0 || i1 > Nx || i1 - i0 < 3) return FDTD_ERR_DIM;
+    if (local_planes) *local_planes = i1 - i0 + 6;
     if (sz) *sz = (Nz + kRowAlign - 1) / kRowAlign * kRowAlign;
     return FDTD_OK;
 }
@@ -223,7 +230,7 @@ FdtdB200Slab* fdtd_b200_slab_create(int Nx, int Ny, int Nz, int i0, int i1, floa
     if (fdtd_b200_slab_layout(Nx, Ny, Nz, i0, i1, &L, &sz) != FDTD_OK || !fields || dx <= 0 || c <= 0)
         return nullptr;
     if ((long long)Nx * Ny * Nz > INT_MAX) return nullptr;
-    for (int q = 0; q < 5; ++q)
+    for (int q = 0; q < 8; ++q)
         if (!fields[q]) return nullptr;
     FdtdB200Slab* h = new FdtdB200Slab();
     if (device < 0) cudaGetDevice(&device);
@@ -233,11 +240,14 @@ FdtdB200Slab* fdtd_b200_slab_create(int Nx, int Ny, int Nz, int i0, int i1, floa
     g.nx = L; g.ny = Ny; g.nz = Nz; g.sz = sz;
     g.plane = (long long)Ny * sz;
     g.cells = (long long)L * g.plane;
-    h->s.x0 = i0 - 2;
+    h->s.x0 = i0 - 3;
     h->s.nxg = Nx;
-    h->s.own_lo = 2;
+    h->s.own_lo = 3;
     h->P[0] = fields[0]; h->P[1] = fields[1];
-    h->V[0] = fields[2]; h->V[1] = fields[3]; h->V[2] = fields[4];
+    for (int c = 0; c < 3; ++c) {
+        h->V[0][c] = fields[2 + c];
+        h->V[1][c] = fields[5 + c];
+    }
     // coefficients exactly as fdtd_create computes them (acoustic_fdtd.cpp:345-349, :1091, :1173)
     const float dt = 0.77f * dx / (c * 1.732050808f);
     h->cf.vc = dt / (rho_air * dx);
@@ -255,7 +265,7 @@ FdtdB200Slab* fdtd_b200_slab_create(int Nx, int Ny, int Nz, int i0, int i1, floa
     float* az = ay + Ny;
     float* px = az + Nz;
     for (int l = 0; l < L; ++l) {
-        const int ig = i0 - 2 + l;
+        const int ig = i0 - 3 + l;
         ax[l] = (ig >= 0 && ig < Nx) ? axis_alpha(ig, Nx, n_pml, dt, a6[0], a6[1]) : 0.0f;
     }
     for (int j = 0; j < Ny; ++j) ay[j] = axis_alpha(j, Ny, n_pml, dt, a6[2], a6[3]);
@@ -287,8 +297,10 @@ void fdtd_b200_slab_destroy(FdtdB200Slab* h)
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     else cudaDeviceSynchronize();
+    if (h->fcache) fused_cache_destroy(h->fcache);
     cudaFree(h->d_tab);
     cudaFree(h->d_bad);
+    cudaFree(h->d_status);
     cudaFree(h->d_sig);
     cudaFree(h->d_ridx);
     cudaFree(h->d_rw);
@@ -306,6 +318,8 @@ int fdtd_b200_slab_set_stream(FdtdB200Slab* h, void* stream)
 float fdtd_b200_slab_dt(const FdtdB200Slab* h) { return h ? h->cf.dt : 0.0f; }
 
 int fdtd_b200_slab_current(const FdtdB200Slab* h) { return h ? h->cur : -1; }
+
+int fdtd_b200_slab_vset(const FdtdB200Slab* h) { return h ? h->cv : -1; }
 
 long long fdtd_b200_slab_launch_count(const FdtdB200Slab* h) { return h ? h->launches : 0; }
 
@@ -364,8 +378,9 @@ int fdtd_b200_slab_deposit(FdtdB200Slab* h, int n)
 int fdtd_b200_slab_velocity(FdtdB200Slab* h)
 {
     if (!h) return FDTD_ERR_NULL;
-    k_slab_vel<<<own_grid(h), dim3(32, 8, 1), 0, h->stream>>>(h->s, h->cf, h->tb, h->P[h->cur], h->V[0],
-                                                             h->V[1], h->V[2]);
+    float* const* v = h->V[h->cv];
+    k_slab_vel<<<own_grid(h), dim3(32, 8, 1), 0, h->stream>>>(h->s, h->cf, h->tb, h->P[h->cur], v[0], v[1],
+                                                             v[2]);
     ++h->launches;
     SCK(cudaGetLastError());
     return FDTD_OK;
@@ -374,11 +389,35 @@ int fdtd_b200_slab_velocity(FdtdB200Slab* h)
 int fdtd_b200_slab_pressure(FdtdB200Slab* h)
 {
     if (!h) return FDTD_ERR_NULL;
+    float* const* v = h->V[h->cv];
     k_slab_pres<<<own_grid(h), dim3(32, 8, 1), 0, h->stream>>>(h->s, h->cf, h->tb, h->P[h->cur],
-                                                              h->P[h->cur ^ 1], h->V[0], h->V[1], h->V[2]);
+                                                              h->P[h->cur ^ 1], v[0], v[1], v[2]);
     ++h->launches;
     SCK(cudaGetLastError());
     h->cur ^= 1;
+    return FDTD_OK;
+}
+
+// One fused step of the own planes: P[cur] -> P[cur^1], V set cv -> cv^1.
+int fdtd_b200_slab_step(FdtdB200Slab* h)
+{
+    if (!h) return FDTD_ERR_NULL;
+    if (!fused_supported(h->s.g)) return FDTD_ERR_DIM;
+    if (!h->fcache) h->fcache = fused_cache_create();
+    if (!h->fcache) return FDTD_ERR_CUDA;
+    if (!h->d_status) {
+        SCK(cudaMalloc(&h->d_status, kStatusWords * sizeof(unsigned)));
+        SCK(cudaMemsetAsync(h->d_status, 0xFF, kStatusWords * sizeof(unsigned), h->stream));
+    }
+    float* const* vi = h->V[h->cv];
+    float* const* vo = h->V[h->cv ^ 1];
+    FusedArgs a{h->s.g, h->cf, h->tb, h->P[h->cur], h->P[h->cur ^ 1], {vi[0], vi[1], vi[2]},
+                {vo[0], vo[1], vo[2]}, h->d_status,
+                XSpan{h->s.x0, h->s.nxg, h->s.own_lo, h->i1 - h->i0}};
+    SCK(launch_fused_step(a, h->fcache, h->stream));
+    ++h->launches;
+    h->cur ^= 1;
+    h->cv ^= 1;
     return FDTD_OK;
 }
 
@@ -394,7 +433,8 @@ int fdtd_b200_slab_record(FdtdB200Slab* h)
 }
 
 // Samples the own cells at global flat indices phase + 1013 t; *bad = the
-// smallest failing index or -1.  Waits for the stream.
+// smallest failing index or -1.  Waits for the stream; also reports a fused
+// step whose load wait ran out (FDTD_ERR_CUDA).
 int fdtd_b200_slab_check(FdtdB200Slab* h, int phase, long long* bad)
 {
     if (!h || !bad) return FDTD_ERR_NULL;
@@ -410,8 +450,15 @@ int fdtd_b200_slab_check(FdtdB200Slab* h, int phase, long long* bad)
         SCK(cudaGetLastError());
     }
     unsigned long long v = 0;
+    unsigned tmo = 0xFFFFFFFFu;
     SCK(cudaMemcpyAsync(&v, h->d_bad, sizeof(v), cudaMemcpyDeviceToHost, h->stream));
+    if (h->d_status)
+        SCK(cudaMemcpyAsync(&tmo, h->d_status + kStatusTimeout, sizeof(tmo), cudaMemcpyDeviceToHost, h->stream));
     SCK(cudaStreamSynchronize(h->stream));
+    if (tmo != 0xFFFFFFFFu) {
+        record_cuda_error(cudaErrorTimeout, "fused slab step: a tile's load wait timed out");
+        return FDTD_ERR_CUDA;
+    }
     *bad = (v == ~0ULL) ? -1 : (long long)v;
     return FDTD_OK;
 }

@@ -1,15 +1,19 @@
 """One room split along i over several ranks (one GPU each): slab decomposition.
 
-Rank r owns the planes ``partition(Nx, world)[r]`` and keeps two ghost planes
-on each side.  One step on every rank:
+Rank r owns the planes ``partition(Nx, world)[r]`` and keeps three ghost
+planes on each side.  One step on every rank, fused schedule (the default):
 
     deposit(n)          source sample n into the local copy of the source cell
                         (owned or ghost: the copies stay identical)
-    velocity()          own faces; reads P on the ghost planes
-    exchange("Vx")      2 planes of Vx to each neighbour
-    pressure()          own cells; reads Vx on the ghost planes
-    exchange("P")       2 planes of the new P to each neighbour
+    step()              the single-pass TMA kernel on the own planes; it
+                        recomputes the Vx faces just outside the slab from
+                        ghost P and ghost old Vx
+    exchange(P, Vx)     3 planes of the new P and 2 of the new Vx to each
+                        neighbour, one batch of point-to-point messages
     record()            receivers whose first tap lies in the own planes
+
+or the two-pass schedule: deposit, velocity, exchange(Vx), pressure,
+exchange(P), record.
 
 and every 256 steps the stability sample of the reference
 (csrc/kernels/acoustic_fdtd.cpp:1245-1268) over the own cells, reduced (min of
@@ -32,14 +36,17 @@ import numpy as np
 from .precision import pressure_taps
 from .rooms import Room
 
-GHOST = 2
+GHOST = 3
+# planes received from the left neighbour (= sent to the right one) and from
+# the right neighbour (= sent to the left one), per exchanged field
+WIDTHS = {"P": (3, 3), "Vx": (2, 2)}
 CHECK_PERIOD, CHECK_STRIDE = 256, 1013
 
 
 def partition(nx: int, world: int) -> List[Tuple[int, int]]:
-    """Contiguous plane ranges, sizes differing by at most one, each >= 2 planes."""
-    if world < 1 or nx < 2 * world:
-        raise ValueError(f"cannot split {nx} planes over {world} ranks (2 planes per rank at least)")
+    """Contiguous plane ranges, sizes differing by at most one, each >= 3 planes."""
+    if world < 1 or nx < 3 * world:
+        raise ValueError(f"cannot split {nx} planes over {world} ranks (3 planes per rank at least)")
     base, rem = divmod(nx, world)
     out, i = [], 0
     for r in range(world):
@@ -57,9 +64,11 @@ def receiver_owner(room: Room, ranges: Sequence[Tuple[int, int]]) -> List[int]:
 
 
 class EngineSlab:
-    """CUDA backend: one fdtd_b200_slab handle over torch-allocated fields."""
+    """CUDA backend: one fdtd_b200_slab handle over torch-allocated fields.
+    fused=True steps with the single-pass kernel, else with the two passes."""
 
-    def __init__(self, room: Room, i0: int, i1: int, rec_ids: Sequence[int], device=None):
+    def __init__(self, room: Room, i0: int, i1: int, rec_ids: Sequence[int], device=None,
+                 fused: bool = True):
         import torch
         from . import _native
         self._native, self._lib = _native, _native.load()
@@ -70,9 +79,10 @@ class EngineSlab:
             raise ValueError(f"slab [{i0}, {i1}) of {room.nx} planes: rc={rc}")
         self.room, self.i0, self.i1, self.own = room, i0, i1, i1 - i0
         self.L, self.sz = L.value, sz.value
+        self.fused = bool(fused)
         self.fields = [torch.zeros((self.L, room.ny, self.sz), dtype=torch.float32, device=self.device)
-                       for _ in range(5)]
-        ptrs = (C.c_void_p * 5)(*[t.data_ptr() for t in self.fields])
+                       for _ in range(8)]
+        ptrs = (C.c_void_p * 8)(*[t.data_ptr() for t in self.fields])
         a6 = np.ascontiguousarray(room.absorption, np.float32)
         h = self._lib.fdtd_b200_slab_create(room.nx, room.ny, room.nz, i0, i1, room.dx, room.c, room.rho,
                                             room.n_pml, a6.ctypes.data_as(_native.P_f32),
@@ -110,10 +120,13 @@ class EngineSlab:
     def field(self, name: str):
         if name == "P":
             return self.fields[self._lib.fdtd_b200_slab_current(self._h)]
-        return self.fields[{"Vx": 2, "Vy": 3, "Vz": 4}[name]]
+        return self.fields[2 + 3 * self._lib.fdtd_b200_slab_vset(self._h) + {"Vx": 0, "Vy": 1, "Vz": 2}[name]]
 
     def deposit(self, n: int):
         self._check(self._lib.fdtd_b200_slab_deposit(self._h, int(n)), "slab_deposit")
+
+    def step(self):
+        self._check(self._lib.fdtd_b200_slab_step(self._h), "slab_step")
 
     def velocity(self):
         self._check(self._lib.fdtd_b200_slab_velocity(self._h), "slab_velocity")
@@ -153,11 +166,13 @@ class LocalExchange:
     def __init__(self, slabs):
         self.slabs = slabs
 
-    def exchange(self, name: str):
-        for a, b in zip(self.slabs[:-1], self.slabs[1:]):
-            fa, fb = a.field(name), b.field(name)
-            fb[0:GHOST].copy_(fa[a.own:a.own + GHOST])
-            fa[a.own + GHOST:a.own + 2 * GHOST].copy_(fb[GHOST:2 * GHOST])
+    def exchange(self, *names: str):
+        for name in names:
+            wl, wr = WIDTHS[name]
+            for a, b in zip(self.slabs[:-1], self.slabs[1:]):
+                fa, fb = a.field(name), b.field(name)
+                fb[GHOST - wl:GHOST].copy_(fa[a.own + GHOST - wl:a.own + GHOST])
+                fa[a.own + GHOST:a.own + GHOST + wr].copy_(fb[GHOST:GHOST + wr])
 
     def reduce_min(self, value: int) -> int:
         return value
@@ -172,16 +187,19 @@ class DistExchange:
     def __init__(self, slab, rank: int, world: int, group=None):
         self.slab, self.rank, self.world, self.group = slab, rank, world, group
 
-    def exchange(self, name: str):
+    def exchange(self, *names: str):
         import torch.distributed as dist
-        t, own = self.slab.field(name), self.slab.own
+        own = self.slab.own
         ops = []
-        if self.rank > 0:
-            ops += [dist.P2POp(dist.isend, t[GHOST:2 * GHOST], self.rank - 1, self.group),
-                    dist.P2POp(dist.irecv, t[0:GHOST], self.rank - 1, self.group)]
-        if self.rank < self.world - 1:
-            ops += [dist.P2POp(dist.isend, t[own:own + GHOST], self.rank + 1, self.group),
-                    dist.P2POp(dist.irecv, t[own + GHOST:own + 2 * GHOST], self.rank + 1, self.group)]
+        for name in names:
+            t = self.slab.field(name)
+            wl, wr = WIDTHS[name]
+            if self.rank > 0:
+                ops += [dist.P2POp(dist.isend, t[GHOST:GHOST + wr], self.rank - 1, self.group),
+                        dist.P2POp(dist.irecv, t[GHOST - wl:GHOST], self.rank - 1, self.group)]
+            if self.rank < self.world - 1:
+                ops += [dist.P2POp(dist.isend, t[own + GHOST - wl:own + GHOST], self.rank + 1, self.group),
+                        dist.P2POp(dist.irecv, t[own + GHOST:own + GHOST + wr], self.rank + 1, self.group)]
         if ops:
             for req in dist.batch_isend_irecv(ops):
                 req.wait()
@@ -208,6 +226,7 @@ class SlabRunner:
     def __init__(self, slabs, exchange):
         self.slabs = list(slabs)
         self.ex = exchange
+        self.fused = all(getattr(s, "fused", False) for s in self.slabs)
         self.step_count = 0
         self.phase = 0
 
@@ -215,12 +234,17 @@ class SlabRunner:
         for _ in range(int(n_steps)):
             for s in self.slabs:
                 s.deposit(self.step_count)
-            for s in self.slabs:
-                s.velocity()
-            self.ex.exchange("Vx")
-            for s in self.slabs:
-                s.pressure()
-            self.ex.exchange("P")
+            if self.fused:
+                for s in self.slabs:
+                    s.step()
+                self.ex.exchange("P", "Vx")
+            else:
+                for s in self.slabs:
+                    s.velocity()
+                self.ex.exchange("Vx")
+                for s in self.slabs:
+                    s.pressure()
+                self.ex.exchange("P")
             for s in self.slabs:
                 s.record()
             self.step_count += 1
@@ -252,19 +276,20 @@ class SlabRunner:
         return np.concatenate([p for _, p in gathered], axis=0)
 
 
-def local_room(room: Room, n_slabs: int, device=None) -> SlabRunner:
+def local_room(room: Room, n_slabs: int, device=None, fused: bool = True) -> SlabRunner:
     """All slabs of a room in this process on one GPU (tests, single-GPU runs)."""
     ranges = partition(room.nx, n_slabs)
     owners = receiver_owner(room, ranges)
-    slabs = [EngineSlab(room, a, b, [q for q, o in enumerate(owners) if o == r], device)
+    slabs = [EngineSlab(room, a, b, [q for q, o in enumerate(owners) if o == r], device, fused)
              for r, (a, b) in enumerate(ranges)]
     return SlabRunner(slabs, LocalExchange(slabs))
 
 
-def distributed_room(room: Room, rank: int, world: int, group=None, device=None) -> SlabRunner:
+def distributed_room(room: Room, rank: int, world: int, group=None, device=None,
+                     fused: bool = True) -> SlabRunner:
     """This rank's slab of a room split over `world` ranks (torch.distributed initialised)."""
     ranges = partition(room.nx, world)
     owners = receiver_owner(room, ranges)
     a, b = ranges[rank]
-    slab = EngineSlab(room, a, b, [q for q, o in enumerate(owners) if o == rank], device)
+    slab = EngineSlab(room, a, b, [q for q, o in enumerate(owners) if o == rank], device, fused)
     return SlabRunner([slab], DistExchange(slab, rank, world, group))

@@ -30,8 +30,9 @@ def _axis(i, n, n_pml, dt, lo, hi):
 
 
 class NumpySlab:
-    def __init__(self, room, i0, i1, rec_ids):
+    def __init__(self, room, i0, i1, rec_ids, fused=False):
         self.room, self.i0, self.i1, self.own = room, i0, i1, i1 - i0
+        self.fused = fused
         self.L = self.own + 2 * GHOST
         self.x0 = i0 - GHOST
         ny, nz = room.ny, room.nz
@@ -85,21 +86,25 @@ class NumpySlab:
         shape[axis] = -1
         return np.where(inner.reshape(shape), g4, g2)
 
-    def velocity(self):
+    def velocity(self, x_lo=None, x_hi=None):
+        """New V of the own planes; x faces on local planes [x_lo, x_hi) (own by default)."""
         room, p = self.room, self.P[self.cur]
         ny, nz, own, x0 = room.ny, room.nz, self.own, self.x0
         lo, hi = GHOST, GHOST + own
+        x_lo = lo if x_lo is None else x_lo
+        x_hi = hi if x_hi is None else x_hi
         ac = self._alpha(slice(lo, hi), slice(0, ny), slice(0, nz))
         dt, vc = self.dt, self.vc
         damp = lambda aL, aR: f32(1) - (f32(0.5) * (aL + aR)) * dt
         vx, vy, vz = self.V
-        # x faces of the own planes that exist globally
-        ig = np.arange(lo, hi) + x0
-        gx = self._grad(p, 0, lo, hi, room.nx, x0)
-        ar = self._alpha(slice(lo + 1, hi + 1), slice(0, ny), slice(0, nz))
-        new = (vx[lo:hi] - vc * gx) * damp(ac, ar)
-        ok = (ig < room.nx - 1)[:, None, None]
-        vx[lo:hi] = np.where(ok, new, vx[lo:hi])
+        # x faces that exist globally
+        ig = np.arange(x_lo, x_hi) + x0
+        gx = self._grad(p, 0, x_lo, x_hi, room.nx, x0)
+        acx = self._alpha(slice(x_lo, x_hi), slice(0, ny), slice(0, nz))
+        ar = self._alpha(slice(x_lo + 1, x_hi + 1), slice(0, ny), slice(0, nz))
+        new = (vx[x_lo:x_hi] - vc * gx) * damp(acx, ar)
+        ok = ((ig >= 0) & (ig < room.nx - 1))[:, None, None]
+        vx[x_lo:x_hi] = np.where(ok, new, vx[x_lo:x_hi])
         # y faces j < ny-1
         gy = self._grad(p[lo:hi], 1, 0, ny - 1, ny, 0)
         ar = self._alpha(slice(lo, hi), slice(1, ny), slice(0, nz))
@@ -107,6 +112,12 @@ class NumpySlab:
         gz = self._grad(p[lo:hi], 2, 0, nz - 1, nz, 0)
         ar = self._alpha(slice(lo, hi), slice(0, ny), slice(1, nz))
         vz[lo:hi, :, : nz - 1] = (vz[lo:hi, :, : nz - 1] - vc * gz) * damp(ac[:, :, : nz - 1], ar)
+
+    def step(self):
+        """The fused kernel's step: x faces two left and one right of the own
+        planes recomputed from ghost P and ghost old Vx, then the pressure."""
+        self.velocity(GHOST - 2, GHOST + self.own + 1)
+        self.pressure()
 
     def pressure(self):
         room, p = self.room, self.P[self.cur]

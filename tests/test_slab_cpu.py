@@ -34,11 +34,11 @@ def test_partition():
     assert partition(10, 3) == [(0, 4), (4, 7), (7, 10)]
     assert partition(512, 8)[-1] == (448, 512)
     with pytest.raises(ValueError):
-        partition(5, 3)
-    for nx, w in [(13, 2), (64, 5), (9, 4)]:
+        partition(8, 3)
+    for nx, w in [(13, 2), (64, 5), (12, 4)]:
         r = partition(nx, w)
         assert r[0][0] == 0 and r[-1][1] == nx
-        assert all(b - a >= 2 for a, b in r) and all(r[q][1] == r[q + 1][0] for q in range(w - 1))
+        assert all(b - a >= 3 for a, b in r) and all(r[q][1] == r[q + 1][0] for q in range(w - 1))
 
 
 def test_receiver_owner():
@@ -47,14 +47,16 @@ def test_receiver_owner():
     assert receiver_owner(room, ranges) == [0, 1, 0, 1]
 
 
+@pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("n_slabs", [1, 2, 4])
-def test_local_slabs_equal_oracle(n_slabs):
+def test_local_slabs_equal_oracle(n_slabs, fused):
     from slab_numpy import NumpySlab
     room = edge_room()
     ranges = partition(room.nx, n_slabs)
     owners = receiver_owner(room, ranges)
-    slabs = [NumpySlab(room, a, b, [q for q, o in enumerate(owners) if o == r])
+    slabs = [NumpySlab(room, a, b, [q for q, o in enumerate(owners) if o == r], fused)
              for r, (a, b) in enumerate(ranges)]
+    assert SlabRunner(slabs, LocalExchange(slabs)).fused == fused
     run = SlabRunner(slabs, LocalExchange(slabs))
     run.step(room.n_steps)
     tr, P = oracle_run(room)
@@ -69,7 +71,7 @@ def _free_port():
         return s.getsockname()[1]
 
 
-def _rank_main(rank, world, port, out_path, nx, steps):
+def _rank_main(rank, world, port, out_path, nx, steps, fused):
     import torch.distributed as dist
     from datetime import timedelta
     from slab_numpy import NumpySlab
@@ -82,7 +84,7 @@ def _rank_main(rank, world, port, out_path, nx, steps):
         ranges = partition(room.nx, world)
         owners = receiver_owner(room, ranges)
         a, b = ranges[rank]
-        slab = NumpySlab(room, a, b, [q for q, o in enumerate(owners) if o == rank])
+        slab = NumpySlab(room, a, b, [q for q, o in enumerate(owners) if o == rank], fused)
         run = SlabRunner([slab], DistExchange(slab, rank, world))
         run.step(room.n_steps)
         tr = run.traces(len(room.receivers))
@@ -93,13 +95,13 @@ def _rank_main(rank, world, port, out_path, nx, steps):
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_gloo_ranks_equal_oracle(world):
+@pytest.mark.parametrize("world,fused", [(2, True), (3, True), (2, False)])
+def test_gloo_ranks_equal_oracle(world, fused):
     import torch.multiprocessing as mp
     room = edge_room(nx=13, steps=140)
     with tempfile.TemporaryDirectory() as d:
         out = os.path.join(d, "r.npz")
-        mp.start_processes(_rank_main, args=(world, _free_port(), out, room.nx, room.n_steps),
+        mp.start_processes(_rank_main, args=(world, _free_port(), out, room.nx, room.n_steps, fused),
                            nprocs=world, join=True, start_method="spawn")
         with np.load(out) as z:
             got_tr, got_P = z["traces"], z["P"]

@@ -1,5 +1,6 @@
 """CUDA slab kernels: a room split into slabs (stepped in one process with
-plane-copy exchanges) equals the whole-room engine bit for bit."""
+plane-copy exchanges), with the fused single-pass kernel or the two passes,
+equals the whole-room engine bit for bit."""
 import numpy as np
 import pytest
 
@@ -31,12 +32,14 @@ def edge_room():
                 (0.3, 0.9, 0.5, 1.0, 0.2, 0.7), "ricker", n_pml=6)
 
 
+@pytest.mark.parametrize("fused", [True, False])
 @pytest.mark.parametrize("n_slabs", [1, 2, 3, 5])
-def test_slabs_equal_whole_room(cuda, n_slabs):
+def test_slabs_equal_whole_room(cuda, n_slabs, fused):
     from spectral_analyzer_b200.slab import local_room
     room = edge_room()
     tr, P = whole(room)
-    run = local_room(room, n_slabs)
+    run = local_room(room, n_slabs, fused=fused)
+    assert run.fused == fused
     run.step(room.n_steps)
     got = run.traces(len(room.receivers))
     assert bits_equal(got, tr), first_mismatch(got, tr)
@@ -44,11 +47,12 @@ def test_slabs_equal_whole_room(cuda, n_slabs):
     assert all(s.launch_count > 0 for s in run.slabs)
 
 
-def test_seeded_room_over_four_slabs(cuda):
+@pytest.mark.parametrize("fused", [True, False])
+def test_seeded_room_over_four_slabs(cuda, fused):
     from spectral_analyzer_b200.slab import local_room
     room = seeded_room(96, 64, 80, 300, seed=21, n_rec=6, n_pml=8)
     tr, P = whole(room)
-    run = local_room(room, 4)
+    run = local_room(room, 4, fused=fused)
     run.step(room.n_steps)
     assert bits_equal(run.traces(6), tr)
     assert bits_equal(run.pressure_field(), P)
