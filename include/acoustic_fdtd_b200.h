@@ -397,6 +397,21 @@ FDTD_B200_API int fdtd_b200_slab_record(FdtdB200Slab* h);
 FDTD_B200_API int fdtd_b200_slab_check(FdtdB200Slab* h, int phase, long long* bad);
 FDTD_B200_API int fdtd_b200_slab_get_traces(FdtdB200Slab* h, float* out, int out_len, int* n_rows);
 
+/* One substep of the reference's uniform co-evolver in one call (no reference
+ * counterpart): fdtd_inject_bridge_drive(st, cell_drives, drive_scale) when
+ * cell_drives is not NULL, fdtd_inject_plate_force(st, n_force, force_idx,
+ * force_wgt, force_total_N) when n_force > 0, fdtd_step(st, 1) and
+ * fdtd_sample_plate_displacement_batch(st, n_saddle, ...), with the same
+ * results and return codes as that sequence (the saddle indices are checked
+ * before stepping) and one stream synchronisation instead of two: the plate
+ * guard of the step is evaluated on the device and read back together with
+ * the saddle samples.  out_saddle_w is written only when the step succeeds. */
+FDTD_B200_API int fdtd_b200_substep(AcousticFDTDState* st, const float* cell_drives,
+                                    float drive_scale, int n_force, const int* force_idx,
+                                    const float* force_wgt, float force_total_N, int n_saddle,
+                                    const int* saddle_idx4, const float* saddle_wgt4,
+                                    float* out_saddle_w);
+
 /* Number of kernels this handle has launched since creation. */
 FDTD_B200_API long long fdtd_b200_launch_count(const AcousticFDTDState* st);
 

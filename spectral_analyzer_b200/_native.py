@@ -112,6 +112,7 @@ SIGNATURES = {
     "fdtd_b200_slab_record": (i32, [vp]),
     "fdtd_b200_slab_check": (i32, [vp, i32, C.POINTER(C.c_longlong)]),
     "fdtd_b200_slab_get_traces": (i32, [vp, P_f32, i32, P_i32]),
+    "fdtd_b200_substep": (i32, [vp, P_f32, f32, i32, P_i32, P_f32, f32, i32, P_i32, P_f32, P_f32]),
     "fdtd_b200_launch_count": (C.c_longlong, [vp]),
     "fdtd_b200_last_error": (C.c_char_p, []),
 }

@@ -1725,3 +1725,150 @@ int fdtd_b200_batch_sync(FdtdB200Batch* b, int* steps_out, int* status_out)
 long long fdtd_b200_batch_launch_count(const FdtdB200Batch* b) { return b ? b->launches : 0; }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- co-evolver substep
+// The uniform co-evolver's per-substep calls (acoustic_coevolver.cpp:2072-2121:
+// fdtd_inject_bridge_drive, fdtd_inject_plate_force, fdtd_step(st, 1),
+// fdtd_sample_plate_displacement_batch) as one call with one stream
+// synchronisation.  With an active plate, fdtd_step must wait for the plate
+// guard before the velocity and pressure updates; here those kernels (and the
+// consumption of the plate forces and the 256-step check) are gated on the
+// device by the plate status word instead, the saddle samples are taken from
+// the new displacement, and the host reads status and samples together.  If
+// the plate update failed, the host undoes its own bookkeeping of the step
+// (buffer rotation, step count, trace row, check phase), which leaves the
+// handle exactly as fdtd_step leaves it on that failure.
+namespace {
+
+int substep_plate(AcousticFDTDState* st, int n_saddle, float* out)
+{
+    cudaStream_t s = st->stream;
+    if (st->ps_n > 0 && st->step_count < st->ps_n && st->ps.n > 0 && st->ps_done_step != st->step_count) {
+        CK(launch_deposit(st->ps, st->d_ps_sig, st->step_count, 0.0f, st->P(), s));
+        ++st->launches;
+        st->ps_done_step = st->step_count;
+    }
+    const bool ext_was_pending = st->ext_pending;
+    if (st->ext_pending) {
+        CK(cudaMemcpyAsync(st->d_ext, st->h_ext, (size_t)st->N_plate * sizeof(float), cudaMemcpyHostToDevice, s));
+        st->dev_ext_nonzero = true;
+    }
+    const unsigned* gate = st->d_status;
+    CK(cudaMemsetAsync(st->d_status + kStatusPlate, 0xFF, sizeof(unsigned), s));
+    CK(launch_plate_step(st->n_act, st->d_act, st->d_nb13, st->d_above, st->d_below, st->d_w[st->wi_cur],
+                         st->d_w[st->wi_prev], st->d_w[st->wi_tmp], st->d_ext, st->P(), st->pc, st->d_status, s));
+    ++st->launches;
+    if (st->dev_ext_nonzero) {
+        CK(launch_zero_gated(st->d_ext, st->N_plate, gate, s));
+        ++st->launches;
+    }
+    // the rest of the step as if the plate update succeeded
+    const int wp0 = st->wi_prev, wc0 = st->wi_cur, wt0 = st->wi_tmp;
+    st->wi_prev = wc0;
+    st->wi_cur = wt0;
+    st->wi_tmp = wp0;
+    CK(launch_velocity_general(st->g, st->cf, st->tb, st->P(), st->V(0), st->V(1), st->V(2), st->d_frac[0],
+                               st->d_frac[1], st->d_frac[2], s, gate));
+    CK(launch_plate_inject(st->n_act, st->d_act, st->d_vzb, st->d_vza, st->d_w[st->wi_cur], st->d_w[st->wi_prev],
+                           st->cf.inv_dt, st->V(2), s, gate));
+    const bool hf = st->has_frac;
+    CK(launch_pressure_general(st->g, st->cf, st->tb, st->P(), st->Pn(), st->V(0), st->V(1), st->V(2),
+                               hf ? st->d_frac[0] : nullptr, hf ? st->d_frac[1] : nullptr,
+                               hf ? st->d_frac[2] : nullptr, st->d_solid, s, gate));
+    st->launches += 3;
+    st->cur ^= 1;
+    ++st->step_count;
+    const int trace0 = st->trace_len;
+    if (st->n_rec > 0 && st->trace_len < st->trace_cap) {
+        CK(launch_wsum(st->P(), st->d_rec_idx, st->d_rec_w, st->n_rec, 8, 0,
+                       st->d_trace + (size_t)st->trace_len * st->n_rec, s));
+        ++st->trace_len;
+        ++st->launches;
+    }
+    const bool checked = (st->step_count & (kCheckPeriod - 1)) == 0;
+    const int phase0 = st->stab_phase;
+    if (checked) {
+        st->stab_phase = (phase0 + 1) % kCheckStride;
+        CK(cudaMemsetAsync(st->d_status + kStatusCell, 0xFF, sizeof(unsigned), s));
+        CK(launch_check(st->g, st->P(), st->N, phase0, st->d_status, st->step_count, s, gate));
+        ++st->launches;
+    }
+    // saddle samples (taps staged by the caller) from the new displacement
+    if (n_saddle > 0) {
+        const size_t n = (size_t)n_saddle * 4;
+        CK(cudaMemcpyAsync(st->d_sidx, st->h_sidx, n * sizeof(long long), cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(st->d_sw, st->h_sw, n * sizeof(float), cudaMemcpyHostToDevice, s));
+        CK(launch_wsum(st->d_w[st->wi_cur], st->d_sidx, st->d_sw, n_saddle, 4, 0, st->d_sout, s));
+        ++st->launches;
+        CK(cudaMemcpyAsync(st->h_sout, st->d_sout, (size_t)n_saddle * sizeof(float), cudaMemcpyDeviceToHost, s));
+    }
+    CK(cudaMemcpyAsync(st->h_status, st->d_status, kStatusWords * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+
+    const unsigned bad = st->h_status[kStatusPlate];
+    if (bad != 0xFFFFFFFFu) {   // the plate guard fired: undo the bookkeeping of the gated step
+        st->cur ^= 1;
+        --st->step_count;
+        st->wi_prev = wp0;
+        st->wi_cur = wc0;
+        st->wi_tmp = wt0;
+        st->trace_len = trace0;
+        if (checked) st->stab_phase = phase0;
+        const int pidx = st->h_act[bad];
+        float wn = NAN;
+        cudaMemcpy(&wn, st->d_w[st->wi_tmp] + pidx, sizeof(float), cudaMemcpyDeviceToHost);
+        fprintf(stderr, "[fdtd_plate] UNSTABLE step=%d plate_node=%d (%d,%d) w_new=%.3g m (limit 0.02 m)\n",
+                st->step_count, pidx, pidx / st->Ny, pidx % st->Ny, (double)wn);
+        fflush(stderr);
+        return FDTD_ERR_UNSTABLE;   // pending forces stay, as after fdtd_step
+    }
+    st->dev_ext_nonzero = false;    // consumed by the gated zeroing
+    if (ext_was_pending) {
+        memset(st->h_ext, 0, (size_t)st->N_plate * sizeof(float));
+        st->ext_pending = false;
+    }
+    if (checked) {
+        if (int rc2 = check_timeout(st)) return rc2;
+        const unsigned cell = st->h_status[kStatusCell];
+        if (cell != 0xFFFFFFFFu) {
+            report_unstable_cell(st, cell);
+            CK(cudaMemsetAsync(st->d_status + kStatusLatch, 0xFF, sizeof(unsigned), s));
+            return FDTD_ERR_UNSTABLE;
+        }
+    }
+    if (n_saddle > 0) memcpy(out, st->h_sout, (size_t)n_saddle * sizeof(float));
+    return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" int fdtd_b200_substep(AcousticFDTDState* st, const float* cell_drives, float drive_scale,
+                                 int n_force, const int* force_idx, const float* force_wgt,
+                                 float force_total_N, int n_saddle, const int* saddle_idx4,
+                                 const float* saddle_wgt4, float* out_saddle_w)
+{
+    if (!st) return FDTD_ERR_NULL;
+    if (n_saddle < 0) return FDTD_ERR_ARG;
+    if (n_saddle > 0 && (!saddle_idx4 || !saddle_wgt4 || !out_saddle_w)) return FDTD_ERR_NULL;
+    for (long long q = 0; q < (long long)n_saddle * 4; ++q)
+        if (saddle_idx4[q] < 0 || saddle_idx4[q] >= st->N_plate) return FDTD_ERR_ARG;
+    if (dev_guard(st)) return FDTD_ERR_CUDA;
+    int rc;
+    if (cell_drives && (rc = fdtd_inject_bridge_drive(st, cell_drives, drive_scale))) return rc;
+    if (n_force > 0 && (rc = fdtd_inject_plate_force(st, n_force, force_idx, force_wgt, force_total_N)))
+        return rc;
+    if (st->n_act == 0) {   // no plate guard: fdtd_step(st, 1) does not wait here
+        if ((rc = one_step(st, true))) return rc;
+        return n_saddle > 0 ? fdtd_sample_plate_displacement_batch(st, n_saddle, saddle_idx4, saddle_wgt4,
+                                                                    out_saddle_w)
+                            : FDTD_OK;
+    }
+    if (n_saddle > 0) {
+        if ((rc = ensure_scratch(st, (size_t)n_saddle * 4))) return rc;
+        for (long long q = 0; q < (long long)n_saddle * 4; ++q) {
+            st->h_sidx[q] = saddle_idx4[q];
+            st->h_sw[q] = saddle_wgt4[q];
+        }
+    }
+    return substep_plate(st, n_saddle, out_saddle_w);
+}

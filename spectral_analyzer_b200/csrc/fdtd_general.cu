@@ -22,103 +22,175 @@ __device__ __forceinline__ float cell_alpha(const Tables& tb, int i, float ay, f
     return fmaxf(fmaxf(__ldg(tb.ax + i), ay), az);
 }
 
+__device__ __forceinline__ float4 ld4(const float* p, long long i) { return *reinterpret_cast<const float4*>(p + i); }
+__device__ __forceinline__ void st4(float* p, long long i, const float (&v)[4])
+{
+    *reinterpret_cast<float4*>(p + i) = make_float4(v[0], v[1], v[2], v[3]);
+}
+__device__ __forceinline__ void unpack(const float4& x, float (&v)[4]) { v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w; }
+
+// Threads own four consecutive cells k0 .. k0+3 of a row (k0 a multiple of 4;
+// rows start on 8-float boundaries, so every float4 access is aligned).
+#define GEN_INDEX                                                          \
+    const int k0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);            \
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;                   \
+    const int i = blockIdx.z;                                              \
+    if (k0 >= g.nz || j >= g.ny) return;                                   \
+    const long long id = ((long long)i * g.ny + j) * g.sz + k0;
+
 // Velocity update on the three staggered face sets (acoustic_fdtd.cpp:1099-1148),
-// then closed faces (fraction == 0) are zeroed (:1152-1154).  One thread per
-// (i, j, k) handles Vx(i+1/2,j,k), Vy(i,j+1/2,k) and Vz(i,j,k+1/2) where they exist.
+// then closed faces (fraction == 0) are zeroed (:1152-1154).  A thread handles
+// Vx(i+1/2,j,k), Vy(i,j+1/2,k) and Vz(i,j,k+1/2) of its four cells where they
+// exist; faces that do not exist (and the row padding) keep their stored zero.
 __global__ void __launch_bounds__(256) k_velocity_general(
     Grid g, Coef cf, Tables tb, const float* __restrict__ p, float* __restrict__ vx,
     float* __restrict__ vy, float* __restrict__ vz, const float* __restrict__ fx,
-    const float* __restrict__ fy, const float* __restrict__ fz)
+    const float* __restrict__ fy, const float* __restrict__ fz, const unsigned* __restrict__ gate)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k >= g.nz || j >= g.ny) return;
-    const long long id = ((long long)i * g.ny + j) * g.sz + k;
-    const float ay = __ldg(tb.ay + j), az = __ldg(tb.az + k);
-    const float ac = cell_alpha(tb, i, ay, az);
-    const float pc = p[id];
-
+    GEN_INDEX
+    if (gate && gate[kStatusPlate] != 0xFFFFFFFFu) return;   // this step's plate update failed
+    const float ay = __ldg(tb.ay + j), axi = __ldg(tb.ax + i);
+    float pc[4], az4[4], ac[4];
+    unpack(ld4(p, id), pc);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        az4[q] = (k0 + q < g.nz) ? __ldg(tb.az + k0 + q) : 0.0f;
+        ac[q] = fmaxf(fmaxf(axi, ay), az4[q]);
+    }
     if (i < g.nx - 1) {
-        const float pr = p[id + g.plane];
-        float grad;
-        if (i > 0 && i < g.nx - 2)
-            grad = fadd(fmul(cf.c1, fsub(pr, pc)),
-                        fmul(cf.c2, fsub(p[id + 2 * g.plane], p[id - g.plane])));
-        else
-            grad = fsub(pr, pc);
-        const float ar = cell_alpha(tb, i + 1, ay, az);
-        float v = fmul(fsub(vx[id], fmul(cf.vc, grad)), face_damp(ac, ar, cf.dt));
-        if (fx && fx[id] == 0.0f) v = 0.0f;
-        vx[id] = v;
+        const bool fourth = i > 0 && i < g.nx - 2;
+        float pr[4], pm[4] = {}, p2[4] = {}, v[4], fr[4] = {1.f, 1.f, 1.f, 1.f};
+        unpack(ld4(p, id + g.plane), pr);
+        if (fourth) {
+            unpack(ld4(p, id - g.plane), pm);
+            unpack(ld4(p, id + 2 * g.plane), p2);
+        }
+        unpack(ld4(vx, id), v);
+        if (fx) unpack(ld4(fx, id), fr);
+        const float axr = __ldg(tb.ax + i + 1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (k0 + q >= g.nz) continue;
+            const float grad = fourth ? fadd(fmul(cf.c1, fsub(pr[q], pc[q])), fmul(cf.c2, fsub(p2[q], pm[q])))
+                                      : fsub(pr[q], pc[q]);
+            float nv = fmul(fsub(v[q], fmul(cf.vc, grad)), face_damp(ac[q], fmaxf(fmaxf(axr, ay), az4[q]), cf.dt));
+            if (fx && fr[q] == 0.0f) nv = 0.0f;
+            v[q] = nv;
+        }
+        st4(vx, id, v);
     }
     if (j < g.ny - 1) {
-        const float pr = p[id + g.sz];
-        float grad;
-        if (j > 0 && j < g.ny - 2)
-            grad = fadd(fmul(cf.c1, fsub(pr, pc)),
-                        fmul(cf.c2, fsub(p[id + 2 * g.sz], p[id - g.sz])));
-        else
-            grad = fsub(pr, pc);
-        const float ar = cell_alpha(tb, i, __ldg(tb.ay + j + 1), az);
-        float v = fmul(fsub(vy[id], fmul(cf.vc, grad)), face_damp(ac, ar, cf.dt));
-        if (fy && fy[id] == 0.0f) v = 0.0f;
-        vy[id] = v;
+        const bool fourth = j > 0 && j < g.ny - 2;
+        float pr[4], pm[4] = {}, p2[4] = {}, v[4], fr[4] = {1.f, 1.f, 1.f, 1.f};
+        unpack(ld4(p, id + g.sz), pr);
+        if (fourth) {
+            unpack(ld4(p, id - g.sz), pm);
+            unpack(ld4(p, id + 2 * g.sz), p2);
+        }
+        unpack(ld4(vy, id), v);
+        if (fy) unpack(ld4(fy, id), fr);
+        const float ayr = __ldg(tb.ay + j + 1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (k0 + q >= g.nz) continue;
+            const float grad = fourth ? fadd(fmul(cf.c1, fsub(pr[q], pc[q])), fmul(cf.c2, fsub(p2[q], pm[q])))
+                                      : fsub(pr[q], pc[q]);
+            float nv = fmul(fsub(v[q], fmul(cf.vc, grad)), face_damp(ac[q], fmaxf(fmaxf(axi, ayr), az4[q]), cf.dt));
+            if (fy && fr[q] == 0.0f) nv = 0.0f;
+            v[q] = nv;
+        }
+        st4(vy, id, v);
     }
-    if (k < g.nz - 1) {
-        const float pr = p[id + 1];
-        float grad;
-        if (k > 0 && k < g.nz - 2)
-            grad = fadd(fmul(cf.c1, fsub(pr, pc)), fmul(cf.c2, fsub(p[id + 2], p[id - 1])));
-        else
-            grad = fsub(pr, pc);
-        const float ar = cell_alpha(tb, i, ay, __ldg(tb.az + k + 1));
-        float v = fmul(fsub(vz[id], fmul(cf.vc, grad)), face_damp(ac, ar, cf.dt));
-        if (fz && fz[id] == 0.0f) v = 0.0f;
-        vz[id] = v;
+    {
+        // P at k0-1 .. k0+5: e[t] = P[k0 - 1 + t]
+        float e[7], v[4], fr[4] = {1.f, 1.f, 1.f, 1.f};
+        e[0] = k0 > 0 ? p[id - 1] : 0.0f;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) e[q + 1] = pc[q];
+        e[5] = k0 + 4 < g.nz ? p[id + 4] : 0.0f;
+        e[6] = k0 + 5 < g.nz ? p[id + 5] : 0.0f;
+        unpack(ld4(vz, id), v);
+        if (fz) unpack(ld4(fz, id), fr);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = k0 + q;
+            if (k >= g.nz - 1) continue;
+            const float grad = (k > 0 && k < g.nz - 2)
+                                   ? fadd(fmul(cf.c1, fsub(e[q + 2], e[q + 1])), fmul(cf.c2, fsub(e[q + 3], e[q])))
+                                   : fsub(e[q + 2], e[q + 1]);
+            float nv = fmul(fsub(v[q], fmul(cf.vc, grad)),
+                            face_damp(ac[q], fmaxf(fmaxf(axi, ay), __ldg(tb.az + k + 1)), cf.dt));
+            if (fz && fr[q] == 0.0f) nv = 0.0f;
+            v[q] = nv;
+        }
+        st4(vz, id, v);
     }
 }
 
 // Pressure update from the 4th-order divergence (acoustic_fdtd.cpp:894-952,
 // :1176-1234).  Faces outside the grid read as zero; with fractions each face
-// is scaled by its open fraction; solid cells are skipped (they stay zero).
+// is scaled by its open fraction; solid cells are skipped (they stay zero in
+// both pressure buffers, so the thread writes zero there).
 __global__ void __launch_bounds__(256) k_pressure_general(
     Grid g, Coef cf, Tables tb, const float* __restrict__ p, float* __restrict__ pn,
     const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz,
     const float* __restrict__ fx, const float* __restrict__ fy, const float* __restrict__ fz,
-    const uint8_t* __restrict__ solid)
+    const uint8_t* __restrict__ solid, const unsigned* __restrict__ gate)
 {
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;
-    const int i = blockIdx.z;
-    if (k >= g.nz || j >= g.ny) return;
-    const long long id = ((long long)i * g.ny + j) * g.sz + k;
-    if (solid && solid[id]) return;
-
-#define FX(q) (fx ? fmul(vx[q], fx[q]) : vx[q])
-#define FY(q) (fy ? fmul(vy[q], fy[q]) : vy[q])
-#define FZ(q) (fz ? fmul(vz[q], fz[q]) : vz[q])
+    GEN_INDEX
+    if (gate && gate[kStatusPlate] != 0xFFFFFFFFu) return;   // this step's plate update failed
     const long long P = g.plane, S = g.sz;
-    const float xp = (i < g.nx - 1) ? FX(id) : 0.0f;
-    const float xm = (i > 0) ? FX(id - P) : 0.0f;
-    const float xpp = (i < g.nx - 2) ? FX(id + P) : 0.0f;
-    const float xmm = (i > 1) ? FX(id - 2 * P) : 0.0f;
-    const float yp = (j < g.ny - 1) ? FY(id) : 0.0f;
-    const float ym = (j > 0) ? FY(id - S) : 0.0f;
-    const float ypp = (j < g.ny - 2) ? FY(id + S) : 0.0f;
-    const float ymm = (j > 1) ? FY(id - 2 * S) : 0.0f;
-    const float zp = (k < g.nz - 1) ? FZ(id) : 0.0f;
-    const float zm = (k > 0) ? FZ(id - 1) : 0.0f;
-    const float zpp = (k < g.nz - 2) ? FZ(id + 1) : 0.0f;
-    const float zmm = (k > 1) ? FZ(id - 2) : 0.0f;
-#undef FX
-#undef FY
-#undef FZ
-    const float d1 = fadd(fadd(fsub(xp, xm), fsub(yp, ym)), fsub(zp, zm));
-    const float d2 = fadd(fadd(fsub(xpp, xmm), fsub(ypp, ymm)), fsub(zpp, zmm));
-    const float dv = fadd(fmul(cf.c1, d1), fmul(cf.c2, d2));
-    const float pd = fminf(fminf(__ldg(tb.px + i), __ldg(tb.py + j)), __ldg(tb.pz + k));
-    pn[id] = fmul(fsub(p[id], fmul(cf.bulk, dv)), pd);
+    // face values times their fractions, four cells at a time (zero when absent)
+    auto face4 = [&](const float* v, const float* f, long long q, bool exists, float (&out)[4]) {
+        if (!exists) {
+            out[0] = out[1] = out[2] = out[3] = 0.0f;
+            return;
+        }
+        unpack(ld4(v, q), out);
+        if (f) {
+            float fr[4];
+            unpack(ld4(f, q), fr);
+#pragma unroll
+            for (int t = 0; t < 4; ++t) out[t] = fmul(out[t], fr[t]);
+        }
+    };
+    float xp[4], xm[4], xpp[4], xmm[4], yp[4], ym[4], ypp[4], ymm[4];
+    face4(vx, fx, id, i < g.nx - 1, xp);
+    face4(vx, fx, id - P, i > 0, xm);
+    face4(vx, fx, id + P, i < g.nx - 2, xpp);
+    face4(vx, fx, id - 2 * P, i > 1, xmm);
+    face4(vy, fy, id, j < g.ny - 1, yp);
+    face4(vy, fy, id - S, j > 0, ym);
+    face4(vy, fy, id + S, j < g.ny - 2, ypp);
+    face4(vy, fy, id - 2 * S, j > 1, ymm);
+    // Vz (times fraction) at k0-2 .. k0+4: e[t] = FZ[k0 - 2 + t]
+    auto fzv = [&](long long q) { return fz ? fmul(vz[q], fz[q]) : vz[q]; };
+    float e[7], c4[4], pc[4], out[4];
+    face4(vz, fz, id, true, c4);
+    e[0] = k0 >= 2 ? fzv(id - 2) : 0.0f;
+    e[1] = k0 >= 1 ? fzv(id - 1) : 0.0f;
+#pragma unroll
+    for (int q = 0; q < 4; ++q) e[q + 2] = c4[q];
+    e[6] = k0 + 4 < g.nz ? fzv(id + 4) : 0.0f;
+    unpack(ld4(p, id), pc);
+    uint32_t sol = 0;
+    if (solid) sol = *reinterpret_cast<const uint32_t*>(solid + id);
+    const float pxy = fminf(__ldg(tb.px + i), __ldg(tb.py + j));
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int k = k0 + q;
+        out[q] = 0.0f;
+        if (k >= g.nz || ((sol >> (8 * q)) & 0xFFu)) continue;
+        const float zp = (k < g.nz - 1) ? e[q + 2] : 0.0f;
+        const float zm = (k > 0) ? e[q + 1] : 0.0f;
+        const float zpp = (k < g.nz - 2) ? e[q + 3] : 0.0f;
+        const float zmm = (k > 1) ? e[q] : 0.0f;
+        const float d1 = fadd(fadd(fsub(xp[q], xm[q]), fsub(yp[q], ym[q])), fsub(zp, zm));
+        const float d2 = fadd(fadd(fsub(xpp[q], xmm[q]), fsub(ypp[q], ymm[q])), fsub(zpp, zmm));
+        const float dv = fadd(fmul(cf.c1, d1), fmul(cf.c2, d2));
+        out[q] = fmul(fsub(pc[q], fmul(cf.bulk, dv)), fminf(pxy, __ldg(tb.pz + k)));
+    }
+    st4(pn, id, out);
 }
 
 // Kirchhoff plate step (acoustic_fdtd.cpp:984-1053), one thread per active node.
@@ -155,10 +227,11 @@ __global__ void k_plate_step(int n_act, const int* __restrict__ act, const int* 
 __global__ void k_plate_inject(int n_act, const int* __restrict__ act,
                                const long long* __restrict__ vzb, const long long* __restrict__ vza,
                                const float* __restrict__ w, const float* __restrict__ wp,
-                               float inv_dt, float* __restrict__ vz)
+                               float inv_dt, float* __restrict__ vz, const unsigned* __restrict__ gate)
 {
     const int q = blockIdx.x * blockDim.x + threadIdx.x;
     if (q >= n_act) return;
+    if (gate && gate[kStatusPlate] != 0xFFFFFFFFu) return;   // this step's plate update failed
     const int pidx = act[q];
     const float v = fmul(fsub(w[pidx], wp[pidx]), inv_dt);
     if (vzb[q] >= 0) vz[vzb[q]] = v;
@@ -196,11 +269,13 @@ __global__ void k_wsum(const float* __restrict__ f, const long long* __restrict_
 // (reference flat order) that are non-finite or beyond +-2e3 Pa record their
 // flat index; the latch keeps the first failing step for async stepping.
 __global__ void k_check(Grid g, const float* __restrict__ p, long long n_cells, int phase,
-                        unsigned* __restrict__ status, int step)
+                        unsigned* __restrict__ status, int step, const unsigned* __restrict__ gate)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long q = phase + t * kCheckStride;
     if (q >= n_cells) return;
+    if (gate && gate[kStatusPlate] != 0xFFFFFFFFu) return;   // this step's plate update failed
+
     const int k = (int)(q % g.nz);
     const long long ij = q / g.nz;
     const int j = (int)(ij % g.ny);
@@ -212,27 +287,37 @@ __global__ void k_check(Grid g, const float* __restrict__ p, long long n_cells, 
     }
 }
 
+
+// Zeroes n floats unless this step's plate update failed (the consumed plate
+// forces of a step whose success is only known after it ran).
+__global__ void k_zero_gated(float* __restrict__ x, int n, const unsigned* __restrict__ gate)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n || gate[kStatusPlate] != 0xFFFFFFFFu) return;
+    x[q] = 0.0f;
+}
 }  // namespace
 
 cudaError_t launch_velocity_general(const Grid& g, const Coef& cf, const Tables& tb,
                                     const float* p, float* vx, float* vy, float* vz,
                                     const float* fx, const float* fy, const float* fz,
-                                    cudaStream_t s)
+                                    cudaStream_t s, const unsigned* gate)
 {
     dim3 block(32, 8, 1);
-    dim3 grid((g.nz + 31) / 32, (g.ny + 7) / 8, g.nx);
-    k_velocity_general<<<grid, block, 0, s>>>(g, cf, tb, p, vx, vy, vz, fx, fy, fz);
+    dim3 grid((g.sz / 4 + 31) / 32, (g.ny + 7) / 8, g.nx);
+    k_velocity_general<<<grid, block, 0, s>>>(g, cf, tb, p, vx, vy, vz, fx, fy, fz, gate);
     return cudaGetLastError();
 }
 
 cudaError_t launch_pressure_general(const Grid& g, const Coef& cf, const Tables& tb,
                                     const float* p, float* pn, const float* vx, const float* vy,
                                     const float* vz, const float* fx, const float* fy,
-                                    const float* fz, const uint8_t* solid, cudaStream_t s)
+                                    const float* fz, const uint8_t* solid, cudaStream_t s,
+                                    const unsigned* gate)
 {
     dim3 block(32, 8, 1);
-    dim3 grid((g.nz + 31) / 32, (g.ny + 7) / 8, g.nx);
-    k_pressure_general<<<grid, block, 0, s>>>(g, cf, tb, p, pn, vx, vy, vz, fx, fy, fz, solid);
+    dim3 grid((g.sz / 4 + 31) / 32, (g.ny + 7) / 8, g.nx);
+    k_pressure_general<<<grid, block, 0, s>>>(g, cf, tb, p, pn, vx, vy, vz, fx, fy, fz, solid, gate);
     return cudaGetLastError();
 }
 
@@ -249,10 +334,10 @@ cudaError_t launch_plate_step(int n_act, const int* act, const int* nb13, const 
 
 cudaError_t launch_plate_inject(int n_act, const int* act, const long long* vzb,
                                 const long long* vza, const float* w, const float* wp,
-                                float inv_dt, float* vz, cudaStream_t s)
+                                float inv_dt, float* vz, cudaStream_t s, const unsigned* gate)
 {
     if (n_act <= 0) return cudaSuccess;
-    k_plate_inject<<<(n_act + 127) / 128, 128, 0, s>>>(n_act, act, vzb, vza, w, wp, inv_dt, vz);
+    k_plate_inject<<<(n_act + 127) / 128, 128, 0, s>>>(n_act, act, vzb, vza, w, wp, inv_dt, vz, gate);
     return cudaGetLastError();
 }
 
@@ -272,12 +357,19 @@ cudaError_t launch_wsum(const float* f, const long long* idx, const float* w, in
 }
 
 cudaError_t launch_check(const Grid& g, const float* p, long long n_cells, int phase,
-                         unsigned* status, int step, cudaStream_t s)
+                         unsigned* status, int step, cudaStream_t s, const unsigned* gate)
 {
     if (phase >= n_cells) return cudaSuccess;
     const long long n = (n_cells - phase + kCheckStride - 1) / kCheckStride;
     const int blocks = (int)((n + 255) / 256);
-    k_check<<<blocks, 256, 0, s>>>(g, p, n_cells, phase, status, step);
+    k_check<<<blocks, 256, 0, s>>>(g, p, n_cells, phase, status, step, gate);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_zero_gated(float* x, int n, const unsigned* gate, cudaStream_t s)
+{
+    if (n <= 0) return cudaSuccess;
+    k_zero_gated<<<(n + 255) / 256, 256, 0, s>>>(x, n, gate);
     return cudaGetLastError();
 }
 

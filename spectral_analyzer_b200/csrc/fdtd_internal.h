@@ -110,24 +110,29 @@ __device__ __forceinline__ float sample8(const float* f, const long long* idx, c
 cudaError_t launch_velocity_general(const Grid& g, const Coef& cf, const Tables& tb,
                                     const float* p, float* vx, float* vy, float* vz,
                                     const float* fx, const float* fy, const float* fz,
-                                    cudaStream_t s);
+                                    cudaStream_t s, const unsigned* gate = nullptr);
 cudaError_t launch_pressure_general(const Grid& g, const Coef& cf, const Tables& tb,
                                     const float* p, float* pn, const float* vx, const float* vy,
                                     const float* vz, const float* fx, const float* fy,
-                                    const float* fz, const uint8_t* solid, cudaStream_t s);
+                                    const float* fz, const uint8_t* solid, cudaStream_t s,
+                                    const unsigned* gate = nullptr);
 cudaError_t launch_plate_step(int n_act, const int* act, const int* nb13, const long long* above,
                               const long long* below, const float* w, const float* wp, float* wt,
                               const float* ext, const float* p, const PlateCoef& pc,
                               unsigned* status, cudaStream_t s);
 cudaError_t launch_plate_inject(int n_act, const int* act, const long long* vzb,
                                 const long long* vza, const float* w, const float* wp,
-                                float inv_dt, float* vz, cudaStream_t s);
+                                float inv_dt, float* vz, cudaStream_t s,
+                                const unsigned* gate = nullptr);
 cudaError_t launch_deposit(const Deposit& d, const float* signal, int step, float amp, float* p,
                            cudaStream_t s);
 cudaError_t launch_wsum(const float* f, const long long* idx, const float* w, int n_out, int taps,
                         int from_zero, float* out, cudaStream_t s);
 cudaError_t launch_check(const Grid& g, const float* p, long long n_cells, int phase,
-                         unsigned* status, int step, cudaStream_t s);
+                         unsigned* status, int step, cudaStream_t s, const unsigned* gate = nullptr);
+// Kernels given a gate (the handle's status words) do nothing once this step's
+// plate update has recorded a failure in gate[kStatusPlate].
+cudaError_t launch_zero_gated(float* x, int n, const unsigned* gate, cudaStream_t s);
 
 // ---- fused single-pass step (fdtd_fused.cu) ----
 // A slab of a room split along i: the local grid holds planes of the global

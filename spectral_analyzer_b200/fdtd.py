@@ -276,6 +276,26 @@ class AcousticFDTD:
                     "sample_plate_displacement_batch")
         return out
 
+    def substep(self, cell_drives=None, drive_scale=1.0, force_idx=None, force_wgt=None,
+                force_total_N=0.0, saddle_idx4=None, saddle_wgt4=None) -> np.ndarray:
+        """One co-evolver substep in one call (fdtd_b200_substep): bridge drive,
+        plate force, one step and the saddle samples, as inject_bridge_drive,
+        inject_plate_force, step(1) and sample_plate_displacement_batch would
+        give them, with one stream synchronisation.  Returns the saddle samples."""
+        drv = _f32(cell_drives) if cell_drives is not None else None
+        fi = _i32(force_idx if force_idx is not None else [])
+        fw = _f32(force_wgt if force_wgt is not None else np.zeros(fi.size), fi.size)
+        si = _i32(saddle_idx4 if saddle_idx4 is not None else [])
+        sw = _f32(saddle_wgt4 if saddle_wgt4 is not None else np.zeros(si.size), si.size)
+        n = si.size // 4
+        out = np.zeros(n, dtype=np.float32)
+        rc = self._check(self._lib.fdtd_b200_substep(
+            self._h, _pf(drv) if drv is not None else None, float(drive_scale), fi.size, _pi(fi), _pf(fw),
+            float(force_total_N), n, _pi(si), _pf(sw), _pf(out)), "substep")
+        if rc == _native.FDTD_ERR_UNSTABLE:
+            raise RuntimeError("AcousticFDTD: pressure diverged (FDTD_ERR_UNSTABLE)")
+        return out
+
     def sample_plate_weighted(self, plate_indices, weights) -> np.float32:
         idx, w = _i32(plate_indices), _f32(weights)
         out = np.zeros(1, dtype=np.float32)
