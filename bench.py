@@ -400,6 +400,12 @@ def engine_arm(args):
     return 0
 
 
+def gpu_uuid(local: int) -> str:
+    import torch
+    g = str(torch.cuda.get_device_properties(local).uuid)
+    return g if g.startswith("GPU-") else "GPU-" + g
+
+
 def serve_arm(args):
     """Serving 256 mixed rooms: Poisson arrivals at serve-load x the sequential capacity."""
     import torch
@@ -416,9 +422,10 @@ def serve_arm(args):
     for r, t in zip(reqs, poisson_arrivals(len(reqs), rate, seed=5)):
         r.arrival = float(t)
     work = request_work(reqs)
-    seq = SequentialServer().run(reqs)
-    srv = BatchServer(max_slots=args.serve_slots, chunk=args.serve_chunk, seg_planes=tune["segment"])
-    bat = srv.run(reqs)
+    with ClockSampler(gpu_uuid(torch.cuda.current_device())) as clk:
+        seq = SequentialServer().run(reqs)
+        srv = BatchServer(max_slots=args.serve_slots, chunk=args.serve_chunk, seg_planes=tune["segment"])
+        bat = srv.run(reqs)
     same = all(np.array_equal(a.traces.view(np.uint32), b.traces.view(np.uint32)) for a, b in zip(seq, bat))
     s_seq, s_bat = summarize(seq, work), summarize(bat, work)
     line = {"metric": "serve requests/s", "value": s_bat["requests_per_s"], "unit": "requests/s",
@@ -432,7 +439,7 @@ def serve_arm(args):
             "batched": s_bat, "sequential": s_seq,
             "speedup_requests_per_s": s_bat["requests_per_s"] / s_seq["requests_per_s"],
             "traces_bit_identical": same, "max_rel_l2_vs_sequential": 0.0 if same else None,
-            "autotune": tune}
+            "autotune": tune, "clocks": clk.summary()}
     print(json.dumps(line), flush=True)
     return 0 if same else 1
 
