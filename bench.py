@@ -424,7 +424,8 @@ def serve_arm(args):
     work = request_work(reqs)
     with ClockSampler(gpu_uuid(torch.cuda.current_device())) as clk:
         seq = SequentialServer().run(reqs)
-        srv = BatchServer(max_slots=args.serve_slots, chunk=args.serve_chunk, seg_planes=tune["segment"])
+        srv = BatchServer(max_slots=args.serve_slots, chunk=args.serve_chunk, seg_planes=tune["segment"],
+                          tile_k=tune["tile"])
         bat = srv.run(reqs)
     same = all(np.array_equal(a.traces.view(np.uint32), b.traces.view(np.uint32)) for a, b in zip(seq, bat))
     s_seq, s_bat = summarize(seq, work), summarize(bat, work)
@@ -435,7 +436,7 @@ def serve_arm(args):
                        "arrivals": "poisson", "offered_load_x_sequential": args.serve_load,
                        "arrival_rate_per_s": rate, "sequential_mean_service_s": service,
                        "slots": args.serve_slots, "chunk_steps": args.serve_chunk,
-                       "segment_planes": tune["segment"]},
+                       "segment_planes": tune["segment"], "tile_k": tune["tile"]},
             "batched": s_bat, "sequential": s_seq,
             "speedup_requests_per_s": s_bat["requests_per_s"] / s_seq["requests_per_s"],
             "traces_bit_identical": same, "max_rel_l2_vs_sequential": 0.0 if same else None,

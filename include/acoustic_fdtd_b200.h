@@ -264,6 +264,10 @@ FDTD_B200_API void fdtd_b200_batch_destroy(FdtdB200Batch* b);
 /* Replace the members; member q advances until its step count reaches limits[q]. */
 FDTD_B200_API int fdtd_b200_batch_set(FdtdB200Batch* b, AcousticFDTDState* const* members,
                                       const int* limits, int n);
+/* Work-item tile: tile_k = 128 (8 rows x 128 columns, the default) or 64
+ * (16 rows x 64 columns, less idle width for rooms with small Nz); takes
+ * effect at the next batch_set. */
+FDTD_B200_API int fdtd_b200_batch_set_tile(FdtdB200Batch* b, int tile_k);
 /* Planes per work item (0 = automatic); takes effect at the next batch_set. */
 FDTD_B200_API int fdtd_b200_batch_set_segment(FdtdB200Batch* b, int planes);
 /* Launch n_steps batched steps without waiting; use_graph = 1 captures them

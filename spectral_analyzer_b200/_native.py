@@ -72,6 +72,7 @@ SIGNATURES = {
     "fdtd_b200_batch_create": (vp, [i32]),
     "fdtd_b200_batch_destroy": (None, [vp]),
     "fdtd_b200_batch_set": (i32, [vp, C.POINTER(vp), P_i32, i32]),
+    "fdtd_b200_batch_set_tile": (i32, [vp, i32]),
     "fdtd_b200_batch_set_segment": (i32, [vp, i32]),
     "fdtd_b200_batch_step": (i32, [vp, i32, i32]),
     "fdtd_b200_batch_sync": (i32, [vp, P_i32, P_i32]),

@@ -1451,7 +1451,10 @@ struct FdtdB200Batch {
     BatchHeader* d_hdr = nullptr;
     unsigned* d_status = nullptr;
     unsigned h_status[kStatusWords];
-    int grid_ctas = 0;
+    int grid_ctas = 0;                   // persistent CTAs of the current tile shape
+    int grid_ctas_shape[2] = {0, 0};
+    int shape = 0;                       // 0: 8 x 128 tiles, 1: 16 x 64 (fdtd_b200_batch_set_tile)
+    int set_shape = 0;                   // the shape the current member set was built with
     int seg_planes = 0;                  // planes per work item, 0 = automatic
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
@@ -1519,7 +1522,8 @@ FdtdB200Batch* fdtd_b200_batch_create(int device)
         cudaMemset(b->d_hdr, 0, sizeof(BatchHeader)) != cudaSuccess ||
         cudaMalloc(&b->d_status, sizeof(unsigned) * kStatusWords) != cudaSuccess ||
         cudaMemset(b->d_status, 0xFF, sizeof(unsigned) * kStatusWords) != cudaSuccess ||
-        fused_batch_slots(&b->grid_ctas) != cudaSuccess) {
+        fused_batch_slots(0, &b->grid_ctas_shape[0]) != cudaSuccess ||
+        fused_batch_slots(1, &b->grid_ctas_shape[1]) != cudaSuccess) {
         set_err(cudaGetLastError(), "fdtd_b200_batch_create");
         fdtd_b200_batch_destroy(b);
         return nullptr;
@@ -1539,6 +1543,15 @@ void fdtd_b200_batch_destroy(FdtdB200Batch* b)
     cudaFree(b->d_status);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
+}
+
+int fdtd_b200_batch_set_tile(FdtdB200Batch* b, int tile_k)
+{
+    if (!b) return FDTD_ERR_NULL;
+    if (tile_k != 128 && tile_k != 64) return FDTD_ERR_ARG;
+    b->shape = tile_k == 64 ? 1 : 0;
+    batch_drop_graph(b);
+    return FDTD_OK;
 }
 
 int fdtd_b200_batch_set_segment(FdtdB200Batch* b, int planes)
@@ -1577,7 +1590,9 @@ int fdtd_b200_batch_set(FdtdB200Batch* b, AcousticFDTDState* const* members, con
         if (st->device != b->device || !fused_eligible(st) || limits[q] < st->step_count) return FDTD_ERR_ARG;
     }
     int tj, tk;
-    fused_tile_shape(&tj, &tk);
+    b->set_shape = b->shape;
+    b->grid_ctas = b->grid_ctas_shape[b->set_shape];
+    fused_tile_shape(b->set_shape, &tj, &tk);
     std::vector<int> item_member;
     for (int q = 0; q < n; ++q) {
         AcousticFDTDState* st = members[q];
@@ -1599,8 +1614,8 @@ int fdtd_b200_batch_set(FdtdB200Batch* b, AcousticFDTDState* const* members, con
         memset(&m, 0, sizeof(m));
         const float* v0[3] = {st->V(0), st->V(1), st->V(2)};
         const float* v1[3] = {st->v[st->cv ^ 1][0], st->v[st->cv ^ 1][1], st->v[st->cv ^ 1][2]};
-        CK(fused_maps(st->fcache, st->g, st->P(), v0, m.maps[0]));
-        CK(fused_maps(st->fcache, st->g, st->Pn(), v1, m.maps[1]));
+        CK(fused_maps(st->fcache, st->g, st->P(), v0, m.maps[0], b->set_shape));
+        CK(fused_maps(st->fcache, st->g, st->Pn(), v1, m.maps[1], b->set_shape));
         m.g = st->g;
         m.cf = st->cf;
         m.tb = st->tb;
@@ -1682,7 +1697,7 @@ int fdtd_b200_batch_step(FdtdB200Batch* b, int n_steps, int use_graph)
     if (!use_graph) {
         for (int s = 0; s < n_steps; ++s) {
             CK(launch_fused_batch_step(b->d_members, b->d_hdr, b->d_item_member, b->d_status,
-                                       b->grid_ctas, b->cap_members, b->stream));
+                                       b->grid_ctas, b->cap_members, b->stream, b->set_shape));
             b->launches += 2;
         }
         return FDTD_OK;
@@ -1694,7 +1709,7 @@ int fdtd_b200_batch_step(FdtdB200Batch* b, int n_steps, int use_graph)
         cudaError_t e = cudaSuccess;
         for (int s = 0; s < n_steps && e == cudaSuccess; ++s)
             e = launch_fused_batch_step(b->d_members, b->d_hdr, b->d_item_member, b->d_status,
-                                        b->grid_ctas, b->cap_members, b->stream);
+                                        b->grid_ctas, b->cap_members, b->stream, b->set_shape);
         cudaError_t e2 = cudaStreamEndCapture(b->stream, &g);
         if (e != cudaSuccess || e2 != cudaSuccess) {
             if (g) cudaGraphDestroy(g);

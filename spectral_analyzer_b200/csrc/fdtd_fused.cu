@@ -49,12 +49,17 @@ namespace fdtd {
 
 namespace {
 
-template <int TJ_, int D_>
+// TJ rows x TK = 4*LW columns per CTA; LW threads per row (float4 each), so a
+// warp covers 32/LW rows.
+template <int TJ_, int D_, int LW_ = 32>
 struct Cfg {
-    static constexpr int TJ = TJ_;              // rows per CTA = warps
-    static constexpr int TK = 128;              // 32 lanes x float4
+    static constexpr int TJ = TJ_;              // rows per CTA
+    static constexpr int LW = LW_;              // threads per row
+    static constexpr int RW = 32 / LW;          // rows per warp
+    static constexpr int TK = 4 * LW;           // columns per CTA
     static constexpr int D = D_;                // prefetch distance (iterations)
-    static constexpr int NT = 32 * TJ;
+    static constexpr int NT = 32 * (TJ / RW);
+    static constexpr int HW = (3 * TJ + 31) / 32;   // warps computing the halo Vz faces
     static constexpr int PR = TJ + 6;           // P box rows j0-3 .. j0+TJ+2
     static constexpr int PC = TK + 8;           // P box cols k0-4 .. k0+TK+3
     static constexpr int RING = D + 4;          // planes u-3 .. u in use + D in flight
@@ -88,7 +93,8 @@ struct Cfg {
     static_assert((PC * 4) % 16 == 0 && (TK * 4) % 16 == 0, "TMA box rows are 16-byte multiples");
     static_assert(PC <= 256 && PR <= 256 && VYR <= 256, "TMA box extent");
     static_assert(VYR <= 2 * TJ, "at most two Vy rows per warp");
-    static_assert(3 * TJ <= 32, "one lane per halo Vz face");
+    static_assert(LW == 32 || LW == 16, "a row is one warp or half a warp");
+    static_assert(TJ % RW == 0 && HW * 32 <= NT, "whole warps of rows; halo warps exist");
 };
 
 constexpr int kWaitSpins = 1 << 21;   // bound on mbarrier polls (each poll may block briefly)
@@ -264,7 +270,9 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
     const Grid g = a.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz, sz = g.sz;
     const long long PL = g.plane;
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    // lane = this thread's float4 column in its row, w = its row in the tile
+    // (with 32 threads per row: the hardware lane and warp)
+    const int tid = threadIdx.x, lane = tid % C::LW, w = tid / C::LW;
     const int tk = tile % tiles_k, tj = tile / tiles_k;
     const int j0 = tj * C::TJ, k0 = tk * C::TK;
     // own planes and the global frame (a slab of a split room, or the whole room)
@@ -500,9 +508,10 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                     sts4(vzn + w * C::PC + 4 * lane + 4, v);
                 }
                 // halo Vz faces k0-2, k0-1, k0+TK of every row: 3*TJ faces, one per
-                // lane of the last warp
-                if (w == C::TJ - 1 && lane < 3 * C::TJ) {
-                    const int jl = lane / 3, which = lane - 3 * jl;
+                // thread of the last HW warps
+                const int hl = tid - (C::NT - 32 * C::HW);
+                if (hl >= 0 && hl < 3 * C::TJ) {
+                    const int jl = hl / 3, which = hl - 3 * jl;
                     const int ch = which < 2 ? 2 + which : C::TK + 4;
                     const int kf = k0 - 4 + ch;
                     const float* prow = pst + (jl + 3) * C::PC;
@@ -689,7 +698,8 @@ __global__ void k_batch_epilogue(BatchMember* __restrict__ mem, const BatchHeade
     }
 }
 
-using FusedCfg = Cfg<8, 2>;
+using FusedCfg = Cfg<8, 2>;          // 8 x 128 tiles: single rooms, and batches by default
+using NarrowCfg = Cfg<16, 2, 16>;    // 16 x 64 tiles: batches of rooms with small Nz
 
 constexpr int kMaxDevices = 64;
 int g_slots_per_sm[kMaxDevices];
@@ -731,7 +741,7 @@ cudaError_t encode_map(CUtensorMap* m, const float* base, const Grid& g, int bx,
 struct FusedCache {
     struct Entry {
         const float* base;
-        int kind;
+        int kind, shape;
         CUtensorMap map;
     };
     std::vector<Entry> entries;
@@ -740,17 +750,28 @@ struct FusedCache {
 FusedCache* fused_cache_create() { return new FusedCache(); }
 void fused_cache_destroy(FusedCache* c) { delete c; }
 
-static cudaError_t cached_map(FusedCache* c, const float* base, int kind, const Grid& g, CUtensorMap* out)
+template <class C>
+void box_of(int kind, int* bx, int* by)
+{
+    const int x[4] = {C::PC, C::TK, C::TK, C::PC};
+    const int y[4] = {C::PR, C::TJ, C::VYR, C::TJ};
+    *bx = x[kind];
+    *by = y[kind];
+}
+
+static cudaError_t cached_map(FusedCache* c, const float* base, int kind, const Grid& g, CUtensorMap* out,
+                              int shape = 0)
 {
     for (const auto& e : c->entries)
-        if (e.base == base && e.kind == kind) { *out = e.map; return cudaSuccess; }
-    using C = FusedCfg;
-    static const int bx[4] = {C::PC, C::TK, C::TK, C::PC};
-    static const int by[4] = {C::PR, C::TJ, C::VYR, C::TJ};
+        if (e.base == base && e.kind == kind && e.shape == shape) { *out = e.map; return cudaSuccess; }
+    int bx, by;
+    if (shape == 1) box_of<NarrowCfg>(kind, &bx, &by);
+    else box_of<FusedCfg>(kind, &bx, &by);
     FusedCache::Entry e;
     e.base = base;
     e.kind = kind;
-    cudaError_t err = encode_map(&e.map, base, g, bx[kind], by[kind]);
+    e.shape = shape;
+    cudaError_t err = encode_map(&e.map, base, g, bx, by);
     if (err != cudaSuccess) return err;
     c->entries.push_back(e);
     *out = e.map;
@@ -809,25 +830,25 @@ cudaError_t launch_fused_step(const FusedArgs& a, FusedCache* cache, cudaStream_
 }
 
 cudaError_t fused_maps(FusedCache* c, const Grid& g, const float* p, const float* const* v,
-                       CUtensorMap out[4])
+                       CUtensorMap out[4], int shape)
 {
     const float* bases[4] = {p, v[0], v[1], v[2]};
     for (int q = 0; q < 4; ++q) {
-        cudaError_t e = cached_map(c, bases[q], q, g, &out[q]);
+        cudaError_t e = cached_map(c, bases[q], q, g, &out[q], shape);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
 
-void fused_tile_shape(int* tj, int* tk)
+void fused_tile_shape(int shape, int* tj, int* tk)
 {
-    *tj = FusedCfg::TJ;
-    *tk = FusedCfg::TK;
+    *tj = shape == 1 ? NarrowCfg::TJ : FusedCfg::TJ;
+    *tk = shape == 1 ? NarrowCfg::TK : FusedCfg::TK;
 }
 
-cudaError_t fused_batch_slots(int* slots)
+template <class C>
+static cudaError_t batch_slots_of(int* slots)
 {
-    using C = FusedCfg;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -843,13 +864,23 @@ cudaError_t fused_batch_slots(int* slots)
     return cudaSuccess;
 }
 
-cudaError_t launch_fused_batch_step(BatchMember* members, BatchHeader* hdr, const int* item_member,
-                                    unsigned* status, int grid_ctas, int epi_blocks, cudaStream_t s)
+cudaError_t fused_batch_slots(int shape, int* slots)
 {
-    using C = FusedCfg;
+    return shape == 1 ? batch_slots_of<NarrowCfg>(slots) : batch_slots_of<FusedCfg>(slots);
+}
+
+cudaError_t launch_fused_batch_step(BatchMember* members, BatchHeader* hdr, const int* item_member,
+                                    unsigned* status, int grid_ctas, int epi_blocks, cudaStream_t s,
+                                    int shape)
+{
     cudaError_t e = cudaMemsetAsync(&hdr->counter, 0, sizeof(int), s);
     if (e != cudaSuccess) return e;
-    k_fused_batch<C><<<grid_ctas, C::NT, C::SMEM_BYTES, s>>>(members, hdr, item_member, status);
+    if (shape == 1)
+        k_fused_batch<NarrowCfg><<<grid_ctas, NarrowCfg::NT, NarrowCfg::SMEM_BYTES, s>>>(members, hdr, item_member,
+                                                                                       status);
+    else
+        k_fused_batch<FusedCfg><<<grid_ctas, FusedCfg::NT, FusedCfg::SMEM_BYTES, s>>>(members, hdr, item_member,
+                                                                                     status);
     e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     k_batch_epilogue<<<epi_blocks, 128, 0, s>>>(members, hdr);

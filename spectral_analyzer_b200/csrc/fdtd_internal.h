@@ -165,7 +165,7 @@ cudaError_t launch_fused_step(const FusedArgs& a, FusedCache* cache, cudaStream_
 int fused_kernel_launches_per_step();
 // TMA descriptors of the four fields a fused step reads (P, Vx, Vy, Vz).
 cudaError_t fused_maps(FusedCache* c, const Grid& g, const float* p, const float* const* v,
-                       CUtensorMap out[4]);
+                       CUtensorMap out[4], int shape = 0);
 
 // ---- batched step (continuous batching of independent rooms) ----
 // Device-resident descriptor of one batch member.  Parity 0 is the member's
@@ -195,9 +195,9 @@ struct alignas(64) BatchMember {
     unsigned unstable;           // first step whose check failed (0xFFFFFFFF = none)
 };
 // Tile geometry of the fused step: rows x columns of a tile.
-void fused_tile_shape(int* tj, int* tk);
+void fused_tile_shape(int shape, int* tj, int* tk);   // shape 0: 8 x 128 tiles, 1: 16 x 64
 // Resident CTAs of the batched kernel on the current device (all SMs).
-cudaError_t fused_batch_slots(int* slots);
+cudaError_t fused_batch_slots(int shape, int* slots);
 // Sizes of the current member set, read by the kernels from device memory so
 // that a captured graph stays valid when the set changes.
 struct BatchHeader {
@@ -210,6 +210,6 @@ struct BatchHeader {
 // receivers, step counter, 256-step check, next source sample).  epi_blocks
 // is the member capacity (blocks beyond n_members exit at once).
 cudaError_t launch_fused_batch_step(BatchMember* members, BatchHeader* hdr, const int* item_member,
-                                    unsigned* status, int grid_ctas, int epi_blocks, cudaStream_t s);
+                                    unsigned* status, int grid_ctas, int epi_blocks, cudaStream_t s, int shape = 0);
 
 }  // namespace fdtd

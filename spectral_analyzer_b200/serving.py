@@ -142,6 +142,10 @@ class EngineBatch:
     def set_segment(self, planes: int):
         self._check(self._lib.fdtd_b200_batch_set_segment(self._h, int(planes)), "batch_set_segment")
 
+    def set_tile(self, tile_k: int):
+        """Work-item tile width: 128 (8 rows) or 64 (16 rows); next set() on."""
+        self._check(self._lib.fdtd_b200_batch_set_tile(self._h, int(tile_k)), "batch_set_tile")
+
     def set(self, solvers, limits):
         n = len(solvers)
         arr = (C.c_void_p * max(n, 1))(*[s._h.value for s in solvers])
@@ -175,13 +179,14 @@ class BatchServer:
     """
 
     def __init__(self, max_slots: int = 64, mem_budget: Optional[int] = None, chunk: int = 64,
-                 use_graph: bool = True, seg_planes: int = 0, backend=None,
+                 use_graph: bool = True, seg_planes: int = 0, tile_k: int = 128, backend=None,
                  clock: Callable[[], float] = time.perf_counter, sleep=time.sleep):
         self.max_slots = max_slots
         self.mem_budget = mem_budget
         self.chunk = chunk
         self.use_graph = use_graph
         self.seg_planes = seg_planes
+        self.tile_k = tile_k
         self.backend = backend or _EngineBackend()
         self.clock = clock
         self.sleep = sleep
@@ -194,6 +199,8 @@ class BatchServer:
         batch = be.batch()
         if self.seg_planes:
             batch.set_segment(self.seg_planes)
+        if self.tile_k != 128:
+            batch.set_tile(self.tile_k)
         active: List[tuple] = []          # (request, solver, start_time)
         used = 0
         results: List[Result] = []

@@ -35,6 +35,9 @@ class FakeBatch:
     def set_segment(self, planes):
         pass
 
+    def set_tile(self, tile_k):
+        pass
+
     def set(self, solvers, limits):
         self.members, self.limits = list(solvers), list(limits)
         self.sets.append(len(solvers))

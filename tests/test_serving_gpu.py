@@ -37,13 +37,14 @@ def alone(room):
     return f.get_traces(), f.get_pressure_field(), f.get_velocity_z()
 
 
-@pytest.mark.parametrize("use_graph", [True, False])
-def test_batch_equals_alone(cuda, use_graph):
+@pytest.mark.parametrize("use_graph,tile_k", [(True, 128), (False, 128), (True, 64), (False, 64)])
+def test_batch_equals_alone(cuda, use_graph, tile_k):
     from spectral_analyzer_b200.serving import EngineBatch, make_solver
     rs = rooms()
     ref = [alone(r) for r in rs]
     solvers = [make_solver(r) for r in rs]
     b = EngineBatch()
+    b.set_tile(tile_k)
     b.set(solvers, [r.n_steps for r in rs])
     steps = np.zeros(len(rs))
     while np.any(steps < [r.n_steps for r in rs]):
@@ -106,7 +107,7 @@ def test_batch_server_matches_sequential(cuda):
     for r, t in zip(reqs, poisson_arrivals(10, rate=400.0, seed=9)):
         r.arrival = float(t)
     seq = SequentialServer().run(reqs)
-    bat = BatchServer(max_slots=6, chunk=32).run(reqs)
+    bat = BatchServer(max_slots=6, chunk=32, tile_k=64).run(reqs)
     for a, b in zip(seq, bat):
         assert a.rid == b.rid
         assert bits_equal(a.traces, b.traces), a.rid
