@@ -702,9 +702,9 @@ using FusedCfg = Cfg<8, 2>;          // 8 x 128 tiles: single rooms, and batches
 using NarrowCfg = Cfg<16, 2, 16>;    // 16 x 64 tiles: batches of rooms with small Nz
 
 constexpr int kMaxDevices = 64;
-int g_slots_per_sm[kMaxDevices];
-int g_sms[kMaxDevices];
-bool g_configured[kMaxDevices];
+int g_slots_per_sm[2][kMaxDevices];   // per tile shape and device
+int g_sms[2][kMaxDevices];
+bool g_configured[2][kMaxDevices];
 
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 std::once_flag g_encode_once;
@@ -785,30 +785,30 @@ bool fused_supported(const Grid& g)
 
 int fused_kernel_launches_per_step() { return 1; }
 
-cudaError_t launch_fused_step(const FusedArgs& a, FusedCache* cache, cudaStream_t s)
+template <class C>
+static cudaError_t launch_step_of(const FusedArgs& a, FusedCache* cache, cudaStream_t s, int shape)
 {
-    using C = FusedCfg;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
-    if (!g_configured[dev]) {
+    if (!g_configured[shape][dev]) {
         e = cudaFuncSetAttribute(k_fused_step<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)C::SMEM_BYTES);
         if (e != cudaSuccess) return e;
-        e = cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev);
+        e = cudaDeviceGetAttribute(&g_sms[shape][dev], cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
         int slots = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&slots, k_fused_step<C>, C::NT, C::SMEM_BYTES);
         if (e != cudaSuccess) return e;
-        g_slots_per_sm[dev] = slots > 0 ? slots : 1;
-        g_configured[dev] = true;
+        g_slots_per_sm[shape][dev] = slots > 0 ? slots : 1;
+        g_configured[shape][dev] = true;
     }
     const Grid& g = a.g;
     CUtensorMap maps[4];
     const float* bases[4] = {a.p, a.vin[0], a.vin[1], a.vin[2]};
     for (int q = 0; q < 4; ++q) {
-        e = cached_map(cache, bases[q], q, g, &maps[q]);
+        e = cached_map(cache, bases[q], q, g, &maps[q], shape);
         if (e != cudaSuccess) return e;
     }
     const int tiles_j = (g.ny + C::TJ - 1) / C::TJ;
@@ -816,7 +816,7 @@ cudaError_t launch_fused_step(const FusedArgs& a, FusedCache* cache, cudaStream_
     const long long tiles = (long long)tiles_j * tiles_k;
     // segments along i: as many as one wave of resident CTAs holds (every CTA
     // marches the same number of planes, so a single full wave has no tail)
-    const long long slots = (long long)g_slots_per_sm[dev] * g_sms[dev];
+    const long long slots = (long long)g_slots_per_sm[shape][dev] * g_sms[shape][dev];
     const int n_own = a.xs.nxg > 0 ? a.xs.n_own : g.nx;
     long long segs = slots / tiles;
     if (segs < 1) segs = 1;
@@ -827,6 +827,20 @@ cudaError_t launch_fused_step(const FusedArgs& a, FusedCache* cache, cudaStream_
     k_fused_step<C><<<grid, C::NT, C::SMEM_BYTES, s>>>(a, maps[0], maps[1], maps[2], maps[3], seg_len,
                                                        tiles_k);
     return cudaGetLastError();
+}
+
+// The tile shape a room's step uses: 16 x 64 tiles when they leave less of the
+// last k tile idle than 8 x 128 tiles (e.g. Nz = 32, 48, 144, 160), else 8 x 128.
+int fused_step_shape(const Grid& g)
+{
+    const int w128 = (g.nz + 127) / 128 * 128 - g.nz, w64 = (g.nz + 63) / 64 * 64 - g.nz;
+    return w64 < w128 ? 1 : 0;
+}
+
+cudaError_t launch_fused_step(const FusedArgs& a, FusedCache* cache, cudaStream_t s)
+{
+    return fused_step_shape(a.g) == 1 ? launch_step_of<NarrowCfg>(a, cache, s, 1)
+                                      : launch_step_of<FusedCfg>(a, cache, s, 0);
 }
 
 cudaError_t fused_maps(FusedCache* c, const Grid& g, const float* p, const float* const* v,
