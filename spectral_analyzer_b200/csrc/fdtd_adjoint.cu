@@ -121,21 +121,154 @@ __device__ __forceinline__ R gradT_cell(const R* w, long long id, long long s, i
     if (k >= g.nz || j >= g.ny) return;                                  \
     const long long id = ((long long)i * g.ny + j) * g.sz + k;
 
+// Four consecutive values at an index that is a multiple of 4 (rows start on
+// 8-element boundaries, so the access is aligned).
+template <class R>
+__device__ __forceinline__ void ld4r(const R* p, long long i, R (&v)[4])
+{
+    if constexpr (sizeof(R) == 4) {
+        const float4 x = *reinterpret_cast<const float4*>(p + i);
+        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
+    } else {
+        const double2 x = *reinterpret_cast<const double2*>(p + i);
+        const double2 y = *reinterpret_cast<const double2*>(p + i + 2);
+        v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
+    }
+}
+template <class R>
+__device__ __forceinline__ void st4r(R* p, long long i, const R (&v)[4])
+{
+    if constexpr (sizeof(R) == 4) {
+        *reinterpret_cast<float4*>(p + i) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+        *reinterpret_cast<double2*>(p + i) = make_double2(v[0], v[1]);
+        *reinterpret_cast<double2*>(p + i + 2) = make_double2(v[2], v[3]);
+    }
+}
+
+// Threads own four consecutive cells k0 .. k0+3 of a row; every per-cell
+// expression below is the scalar one of the helpers above, in the same order.
+#define ADJ4_INDEX                                                       \
+    const int k0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);          \
+    const int j = blockIdx.y * blockDim.y + threadIdx.y;                 \
+    const int i = blockIdx.z;                                            \
+    if (k0 >= g.nz || j >= g.ny) return;                                 \
+    const long long id = ((long long)i * g.ny + j) * g.sz + k0;
+
+// Gradient on the faces of the four cells along x or y (stride s, face index f,
+// n cells on that axis): grad_face for each cell.
+template <class R>
+__device__ __forceinline__ void grad4(const R* p, long long id, long long s, int f, int n, const ACoef<R>& cf,
+                                      const R (&pc)[4], R (&gr)[4])
+{
+    R pr[4], pm[4], p2[4];
+    ld4r(p, id + s, pr);
+    if (f > 0 && f < n - 2) {
+        ld4r(p, id - s, pm);
+        ld4r(p, id + 2 * s, p2);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) gr[q] = radd(rmul(cf.c1, rsub(pr[q], pc[q])), rmul(cf.c2, rsub(p2[q], pm[q])));
+    } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) gr[q] = rsub(pr[q], pc[q]);
+    }
+}
+
+// P (or any cell field) at k0-1 .. k0+5: e[t] = f[k0 - 1 + t], zero outside the row.
+template <class R>
+__device__ __forceinline__ void zrow(const R* f, long long id, int k0, int nz, const R (&c)[4], R (&e)[7])
+{
+    e[0] = k0 > 0 ? f[id - 1] : R(0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) e[q + 1] = c[q];
+    e[5] = k0 + 4 < nz ? f[id + 4] : R(0);
+    e[6] = k0 + 5 < nz ? f[id + 5] : R(0);
+}
+
+// z-face gradient of cell k = k0+q from e (zrow of P): grad_face along z.
+template <class R>
+__device__ __forceinline__ R gradz(const R (&e)[7], int q, int k, int nz, const ACoef<R>& cf)
+{
+    if (k > 0 && k < nz - 2) return radd(rmul(cf.c1, rsub(e[q + 2], e[q + 1])), rmul(cf.c2, rsub(e[q + 3], e[q])));
+    return rsub(e[q + 2], e[q + 1]);
+}
+
+// Divergence of the four cells (div_cell for each).
+template <class R>
+__device__ __forceinline__ void div4(const Grid& g, const R* vx, const R* vy, const R* vz, long long id, int i,
+                                     int j, int k0, const ACoef<R>& cf, R (&dv)[4])
+{
+    const long long P = g.plane, S = g.sz;
+    R xp[4] = {}, xm[4] = {}, xpp[4] = {}, xmm[4] = {}, yp[4] = {}, ym[4] = {}, ypp[4] = {}, ymm[4] = {};
+    if (i < g.nx - 1) ld4r(vx, id, xp);
+    if (i > 0) ld4r(vx, id - P, xm);
+    if (i < g.nx - 2) ld4r(vx, id + P, xpp);
+    if (i > 1) ld4r(vx, id - 2 * P, xmm);
+    if (j < g.ny - 1) ld4r(vy, id, yp);
+    if (j > 0) ld4r(vy, id - S, ym);
+    if (j < g.ny - 2) ld4r(vy, id + S, ypp);
+    if (j > 1) ld4r(vy, id - 2 * S, ymm);
+    R zc[4], ez[7];   // ez[t] = Vz[k0 - 2 + t]
+    ld4r(vz, id, zc);
+    ez[0] = k0 >= 2 ? vz[id - 2] : R(0);
+    ez[1] = k0 >= 1 ? vz[id - 1] : R(0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ez[q + 2] = zc[q];
+    ez[6] = k0 + 4 < g.nz ? vz[id + 4] : R(0);
+    const R z0 = R(0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int k = k0 + q;
+        const R zp = (k < g.nz - 1) ? ez[q + 2] : z0, zm = (k > 0) ? ez[q + 1] : z0;
+        const R zpp = (k < g.nz - 2) ? ez[q + 3] : z0, zmm = (k > 1) ? ez[q] : z0;
+        const R d1 = radd(radd(rsub(xp[q], xm[q]), rsub(yp[q], ym[q])), rsub(zp, zm));
+        const R d2 = radd(radd(rsub(xpp[q], xmm[q]), rsub(ypp[q], ymm[q])), rsub(zpp, zmm));
+        dv[q] = radd(rmul(cf.c1, d1), rmul(cf.c2, d2));
+    }
+}
+
 template <class R>
 __global__ void __launch_bounds__(256) k_fwd_vel(Grid g, ACoef<R> cf, const R* __restrict__ a,
                                                  const R* __restrict__ p, const R* vin0, const R* vin1,
                                                  const R* vin2, R* vout0, R* vout1, R* vout2)
 {
-    ADJ_INDEX
-    const R ac = a[id];
-    if (i < g.nx - 1)
-        vout0[id] = rmul(rsub(vin0[id], rmul(cf.vc, grad_face(p, id, g.plane, i, g.nx, cf))),
-                         face_d(ac, a[id + g.plane]));
-    if (j < g.ny - 1)
-        vout1[id] = rmul(rsub(vin1[id], rmul(cf.vc, grad_face(p, id, (long long)g.sz, j, g.ny, cf))),
-                         face_d(ac, a[id + g.sz]));
-    if (k < g.nz - 1)
-        vout2[id] = rmul(rsub(vin2[id], rmul(cf.vc, grad_face(p, id, 1LL, k, g.nz, cf))), face_d(ac, a[id + 1]));
+    ADJ4_INDEX
+    R ac[4], pc[4];
+    ld4r(a, id, ac);
+    ld4r(p, id, pc);
+    if (i < g.nx - 1) {
+        R gr[4], ar[4], v[4];
+        grad4(p, id, g.plane, i, g.nx, cf, pc, gr);
+        ld4r(a, id + g.plane, ar);
+        ld4r(vin0, id, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (k0 + q < g.nz) v[q] = rmul(rsub(v[q], rmul(cf.vc, gr[q])), face_d(ac[q], ar[q]));
+        st4r(vout0, id, v);
+    }
+    if (j < g.ny - 1) {
+        R gr[4], ar[4], v[4];
+        grad4(p, id, (long long)g.sz, j, g.ny, cf, pc, gr);
+        ld4r(a, id + g.sz, ar);
+        ld4r(vin1, id, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (k0 + q < g.nz) v[q] = rmul(rsub(v[q], rmul(cf.vc, gr[q])), face_d(ac[q], ar[q]));
+        st4r(vout1, id, v);
+    }
+    {
+        R e[7], v[4];
+        zrow(p, id, k0, g.nz, pc, e);
+        const R a4 = k0 + 4 < g.nz ? a[id + 4] : R(0);
+        ld4r(vin2, id, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = k0 + q;
+            if (k < g.nz - 1)
+                v[q] = rmul(rsub(v[q], rmul(cf.vc, gradz(e, q, k, g.nz, cf))), face_d(ac[q], q < 3 ? ac[q + 1] : a4));
+        }
+        st4r(vout2, id, v);
+    }
 }
 
 template <class R>
@@ -144,9 +277,15 @@ __global__ void __launch_bounds__(256) k_fwd_pres(Grid g, ACoef<R> cf, const R* 
                                                   const R* __restrict__ vy, const R* __restrict__ vz,
                                                   R* __restrict__ pn)
 {
-    ADJ_INDEX
-    const R dv = div_cell(g, vx, vy, vz, id, i, j, k, cf);
-    pn[id] = rmul(rsub(p[id], rmul(cf.bulk, dv)), cell_q(a[id]));
+    ADJ4_INDEX
+    R dv[4], pc[4], ac[4], out[4];
+    div4(g, vx, vy, vz, id, i, j, k0, cf, dv);
+    ld4r(p, id, pc);
+    ld4r(a, id, ac);
+#pragma unroll
+    for (int q = 0; q < 4; ++q)
+        out[q] = (k0 + q < g.nz) ? rmul(rsub(pc[q], rmul(cf.bulk, dv[q])), cell_q(ac[q])) : R(0);
+    st4r(pn, id, out);
 }
 
 // Source deposit into the (open) source cell before step n.
@@ -176,6 +315,9 @@ __global__ void k_inject(R* lp, int n_rec, const long long* idx, const R* w, con
         for (int t = 0; t < 8; ++t) lp[idx[8 * r + t]] = radd(lp[idx[8 * r + t]], rmul(w[8 * r + t], rrow[r]));
 }
 
+__device__ __forceinline__ void ld4d(const double* p, long long i, double (&v)[4]) { ld4r<double>(p, i, v); }
+__device__ __forceinline__ void st4d(double* p, long long i, const double (&v)[4]) { st4r<double>(p, i, v); }
+
 template <class R>
 __global__ void __launch_bounds__(256) k_adj_cells1(Grid g, ACoef<R> cf, const R* __restrict__ a,
                                                     const R* __restrict__ lam, const R* __restrict__ pt,
@@ -183,12 +325,39 @@ __global__ void __launch_bounds__(256) k_adj_cells1(Grid g, ACoef<R> cf, const R
                                                     const R* __restrict__ vz, R* __restrict__ u,
                                                     double* __restrict__ grad)
 {
-    ADJ_INDEX
-    const R q = cell_q(a[id]);
-    const R l = lam[id];
-    u[id] = rmul(l, q);
-    const R z = rsub(pt[id], rmul(cf.bulk, div_cell(g, vx, vy, vz, id, i, j, k, cf)));
-    grad[id] -= (double)q * (double)q * (double)l * (double)z;
+    ADJ4_INDEX
+    R ac[4], l[4], ptc[4], dv[4], uo[4];
+    double gr[4];
+    ld4r(a, id, ac);
+    ld4r(lam, id, l);
+    ld4r(pt, id, ptc);
+    div4(g, vx, vy, vz, id, i, j, k0, cf, dv);
+    ld4d(grad, id, gr);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        uo[q] = R(0);
+        if (k0 + q >= g.nz) continue;
+        const R qq = cell_q(ac[q]);
+        uo[q] = rmul(l[q], qq);
+        const R z = rsub(ptc[q], rmul(cf.bulk, dv[q]));
+        gr[q] -= (double)qq * (double)qq * (double)l[q] * (double)z;
+    }
+    st4r(u, id, uo);
+    st4d(grad, id, gr);
+}
+
+// Transposed divergence on the x or y faces of the four cells (divT_face each).
+template <class R>
+__device__ __forceinline__ void divT4(const R* u, long long id, long long s, int f, int n, const ACoef<R>& cf,
+                                      R (&out)[4])
+{
+    R uc[4], ur[4], um[4] = {}, upp[4] = {};
+    ld4r(u, id, uc);
+    ld4r(u, id + s, ur);
+    if (f >= 1) ld4r(u, id - s, um);
+    if (f <= n - 3) ld4r(u, id + 2 * s, upp);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) out[q] = radd(rmul(cf.c1, rsub(uc[q], ur[q])), rmul(cf.c2, rsub(um[q], upp[q])));
 }
 
 template <class R>
@@ -198,26 +367,96 @@ __global__ void __launch_bounds__(256) k_adj_faces(Grid g, ACoef<R> cf, const R*
                                                    const R* __restrict__ vo2, R* lv0, R* lv1, R* lv2,
                                                    R* __restrict__ e0, R* __restrict__ e1, R* __restrict__ e2)
 {
-    ADJ_INDEX
-    const R ac = a[id];
-    if (i < g.nx - 1) {
-        const R mu = rsub(lv0[id], rmul(cf.bulk, divT_face(u, id, g.plane, i, g.nx, cf)));
-        const R y = rsub(vo0[id], rmul(cf.vc, grad_face(pt, id, g.plane, i, g.nx, cf)));
-        lv0[id] = rmul(mu, face_d(ac, a[id + g.plane]));
-        e0[id] = rmul(mu, y);
+    ADJ4_INDEX
+    R ac[4], ptc[4];
+    ld4r(a, id, ac);
+    ld4r(pt, id, ptc);
+    // x and y faces
+#pragma unroll
+    for (int ax = 0; ax < 2; ++ax) {
+        const bool exists = ax == 0 ? i < g.nx - 1 : j < g.ny - 1;
+        if (!exists) continue;
+        const long long s = ax == 0 ? g.plane : (long long)g.sz;
+        const int f = ax == 0 ? i : j, n = ax == 0 ? g.nx : g.ny;
+        R* lv = ax == 0 ? lv0 : lv1;
+        R* ef = ax == 0 ? e0 : e1;
+        const R* vo = ax == 0 ? vo0 : vo1;
+        R dt[4], gr[4], ar[4], l[4], v[4], eo[4];
+        divT4(u, id, s, f, n, cf, dt);
+        grad4(pt, id, s, f, n, cf, ptc, gr);
+        ld4r(a, id + s, ar);
+        ld4r(lv, id, l);
+        ld4r(vo, id, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            eo[q] = R(0);
+            if (k0 + q >= g.nz) continue;
+            const R mu = rsub(l[q], rmul(cf.bulk, dt[q]));
+            const R y = rsub(v[q], rmul(cf.vc, gr[q]));
+            l[q] = rmul(mu, face_d(ac[q], ar[q]));
+            eo[q] = rmul(mu, y);
+        }
+        st4r(lv, id, l);
+        st4r(ef, id, eo);
     }
-    if (j < g.ny - 1) {
-        const long long s = g.sz;
-        const R mu = rsub(lv1[id], rmul(cf.bulk, divT_face(u, id, s, j, g.ny, cf)));
-        const R y = rsub(vo1[id], rmul(cf.vc, grad_face(pt, id, s, j, g.ny, cf)));
-        lv1[id] = rmul(mu, face_d(ac, a[id + s]));
-        e1[id] = rmul(mu, y);
+    // z faces: U and P at k0-1 .. k0+5, a at k0 .. k0+4
+    {
+        R uc[4], eu[7], ep[7], l[4], v[4], eo[4];
+        ld4r(u, id, uc);
+        zrow(u, id, k0, g.nz, uc, eu);
+        zrow(pt, id, k0, g.nz, ptc, ep);
+        const R a4 = k0 + 4 < g.nz ? a[id + 4] : R(0);
+        ld4r(lv2, id, l);
+        ld4r(vo2, id, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int k = k0 + q;
+            eo[q] = R(0);
+            if (k >= g.nz - 1) continue;
+            // divT_face along z: c1 (u[k] - u[k+1]) + c2 (u[k-1] - u[k+2]), zero outside
+            const R um = k >= 1 ? eu[q] : R(0), upp = k <= g.nz - 3 ? eu[q + 3] : R(0);
+            const R dt = radd(rmul(cf.c1, rsub(eu[q + 1], eu[q + 2])), rmul(cf.c2, rsub(um, upp)));
+            const R mu = rsub(l[q], rmul(cf.bulk, dt));
+            const R y = rsub(v[q], rmul(cf.vc, gradz(ep, q, k, g.nz, cf)));
+            l[q] = rmul(mu, face_d(ac[q], q < 3 ? ac[q + 1] : a4));
+            eo[q] = rmul(mu, y);
+        }
+        st4r(lv2, id, l);
+        st4r(e2, id, eo);
     }
-    if (k < g.nz - 1) {
-        const R mu = rsub(lv2[id], rmul(cf.bulk, divT_face(u, id, 1LL, k, g.nz, cf)));
-        const R y = rsub(vo2[id], rmul(cf.vc, grad_face(pt, id, 1LL, k, g.nz, cf)));
-        lv2[id] = rmul(mu, face_d(ac, a[id + 1]));
-        e2[id] = rmul(mu, y);
+}
+
+// Transposed gradient of the four cells along x or y (cell index t uniform).
+template <class R>
+__device__ __forceinline__ void gradT4(const R* w, long long id, long long s, int t, int n, const ACoef<R>& cf,
+                                       R (&out)[4])
+{
+    const int nf = n - 1;
+    auto inner = [&](int f) { return f > 0 && f < n - 2; };
+#pragma unroll
+    for (int q = 0; q < 4; ++q) out[q] = R(0);
+    R v[4];
+    if (t - 1 >= 0 && t - 1 < nf) {
+        ld4r(w, id - s, v);
+        const R c = inner(t - 1) ? cf.c1 : R(1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out[q] = radd(out[q], rmul(c, v[q]));
+    }
+    if (t < nf) {
+        ld4r(w, id, v);
+        const R c = inner(t) ? cf.c1 : R(1);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out[q] = rsub(out[q], rmul(c, v[q]));
+    }
+    if (t - 2 >= 0 && inner(t - 2)) {
+        ld4r(w, id - 2 * s, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out[q] = radd(out[q], rmul(cf.c2, v[q]));
+    }
+    if (t + 1 < nf && inner(t + 1)) {
+        ld4r(w, id + s, v);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) out[q] = rsub(out[q], rmul(cf.c2, v[q]));
     }
 }
 
@@ -228,20 +467,57 @@ __global__ void __launch_bounds__(256) k_adj_cells2(Grid g, ACoef<R> cf, const R
                                                     const R* __restrict__ e1, const R* __restrict__ e2,
                                                     R* __restrict__ lp, double* __restrict__ grad)
 {
-    ADJ_INDEX
+    ADJ4_INDEX
     const long long P = g.plane, S = g.sz;
-    R gt = gradT_cell(w0, id, P, i, g.nx, cf);
-    gt = radd(gt, gradT_cell(w1, id, S, j, g.ny, cf));
-    gt = radd(gt, gradT_cell(w2, id, 1LL, k, g.nz, cf));
-    lp[id] = rsub(u[id], rmul(cf.vc, gt));
-    double e = 0.0;
-    if (i < g.nx - 1) e += (double)e0[id];
-    if (i > 0) e += (double)e0[id - P];
-    if (j < g.ny - 1) e += (double)e1[id];
-    if (j > 0) e += (double)e1[id - S];
-    if (k < g.nz - 1) e += (double)e2[id];
-    if (k > 0) e += (double)e2[id - 1];
-    grad[id] -= 0.5 * e;
+    R gx[4], gy[4], uc[4], wc[4], ew[7], lo[4];
+    gradT4(w0, id, P, i, g.nx, cf, gx);
+    gradT4(w1, id, S, j, g.ny, cf, gy);
+    ld4r(u, id, uc);
+    // W_z at k0-2 .. k0+4: ew[t] = Wz[k0 - 2 + t]
+    ld4r(w2, id, wc);
+    ew[0] = k0 >= 2 ? w2[id - 2] : R(0);
+    ew[1] = k0 >= 1 ? w2[id - 1] : R(0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ew[q + 2] = wc[q];
+    ew[6] = k0 + 4 < g.nz ? w2[id + 4] : R(0);
+    // E: x and y faces of the four cells, and the z faces k0-1 .. k0+3
+    R ex[4] = {}, exm[4] = {}, ey[4] = {}, eym[4] = {}, ezc[4], ez[5];
+    if (i < g.nx - 1) ld4r(e0, id, ex);
+    if (i > 0) ld4r(e0, id - P, exm);
+    if (j < g.ny - 1) ld4r(e1, id, ey);
+    if (j > 0) ld4r(e1, id - S, eym);
+    ld4r(e2, id, ezc);
+    ez[0] = k0 >= 1 ? e2[id - 1] : R(0);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) ez[q + 1] = ezc[q];
+    double gr[4];
+    ld4d(grad, id, gr);
+    const int nzf = g.nz - 1;
+    auto innerz = [&](int f) { return f > 0 && f < g.nz - 2; };
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int k = k0 + q;
+        lo[q] = R(0);
+        if (k >= g.nz) continue;
+        // gradT_cell along z, term order of the scalar helper
+        R gz = R(0);
+        if (k - 1 >= 0 && k - 1 < nzf) gz = radd(gz, rmul(innerz(k - 1) ? cf.c1 : R(1), ew[q + 1]));
+        if (k < nzf) gz = rsub(gz, rmul(innerz(k) ? cf.c1 : R(1), ew[q + 2]));
+        if (k - 2 >= 0 && innerz(k - 2)) gz = radd(gz, rmul(cf.c2, ew[q]));
+        if (k + 1 < nzf && innerz(k + 1)) gz = rsub(gz, rmul(cf.c2, ew[q + 3]));
+        R gt = radd(radd(gx[q], gy[q]), gz);
+        lo[q] = rsub(uc[q], rmul(cf.vc, gt));
+        double e = 0.0;
+        if (i < g.nx - 1) e += (double)ex[q];
+        if (i > 0) e += (double)exm[q];
+        if (j < g.ny - 1) e += (double)ey[q];
+        if (j > 0) e += (double)eym[q];
+        if (k < g.nz - 1) e += (double)ez[q + 1];
+        if (k > 0) e += (double)ez[q];
+        gr[q] -= 0.5 * e;
+    }
+    st4r(lp, id, lo);
+    st4d(grad, id, gr);
 }
 
 // a (reference order, float or double) -> padded R array
@@ -329,6 +605,7 @@ void dfree(FdtdB200Adj* h, void*& p)
 size_t field_bytes(const FdtdB200Adj* h) { return (size_t)h->g.cells * h->eb; }
 
 dim3 cell_grid(const Grid& g) { return dim3((g.nz + 31) / 32, (g.ny + 7) / 8, g.nx); }
+dim3 vec_grid(const Grid& g) { return dim3((g.sz / 4 + 31) / 32, (g.ny + 7) / 8, g.nx); }   // four cells per thread
 const dim3 kBlock(32, 8, 1);
 
 template <class R>
@@ -348,10 +625,10 @@ void fwd_step(FdtdB200Adj* h, int n, void* p, void* const* vin, void* const* vou
         k_deposit<R><<<1, 1, 0, h->stream>>>((R*)p, h->src, (const R*)h->sig, n);
         ++h->launches;
     }
-    k_fwd_vel<R><<<cell_grid(g), kBlock, 0, h->stream>>>(g, cf, (const R*)h->a, (const R*)p, (const R*)vin[0],
+    k_fwd_vel<R><<<vec_grid(g), kBlock, 0, h->stream>>>(g, cf, (const R*)h->a, (const R*)p, (const R*)vin[0],
                                                          (const R*)vin[1], (const R*)vin[2], (R*)vout[0],
                                                          (R*)vout[1], (R*)vout[2]);
-    k_fwd_pres<R><<<cell_grid(g), kBlock, 0, h->stream>>>(g, cf, (const R*)h->a, (const R*)p, (const R*)vout[0],
+    k_fwd_pres<R><<<vec_grid(g), kBlock, 0, h->stream>>>(g, cf, (const R*)h->a, (const R*)p, (const R*)vout[0],
                                                           (const R*)vout[1], (const R*)vout[2], (R*)pn);
     h->launches += 2;
     if (h->n_rec > 0 && n < h->trace_cap) {
@@ -515,14 +792,14 @@ int backward_impl(FdtdB200Adj* h)
                                                     (const R*)h->resid + (size_t)n * h->n_rec);
                 ++h->launches;
             }
-            k_adj_cells1<R><<<cell_grid(g), kBlock, 0, h->stream>>>(
+            k_adj_cells1<R><<<vec_grid(g), kBlock, 0, h->stream>>>(
                 g, cf, (const R*)h->a, (const R*)h->Lp, (const R*)h->sP[t], (const R*)vn[0], (const R*)vn[1],
                 (const R*)vn[2], (R*)h->U, h->grad);
-            k_adj_faces<R><<<cell_grid(g), kBlock, 0, h->stream>>>(
+            k_adj_faces<R><<<vec_grid(g), kBlock, 0, h->stream>>>(
                 g, cf, (const R*)h->a, (const R*)h->U, (const R*)h->sP[t], (const R*)vo[0], (const R*)vo[1],
                 (const R*)vo[2], (R*)h->Lv[0], (R*)h->Lv[1], (R*)h->Lv[2], (R*)h->E[0], (R*)h->E[1],
                 (R*)h->E[2]);
-            k_adj_cells2<R><<<cell_grid(g), kBlock, 0, h->stream>>>(
+            k_adj_cells2<R><<<vec_grid(g), kBlock, 0, h->stream>>>(
                 g, cf, (const R*)h->U, (const R*)h->Lv[0], (const R*)h->Lv[1], (const R*)h->Lv[2],
                 (const R*)h->E[0], (const R*)h->E[1], (const R*)h->E[2], (R*)h->Lp, h->grad);
             h->launches += 3;
