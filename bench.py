@@ -73,6 +73,8 @@ def parse_args():
     ap.add_argument("--decompose", action="store_true",
                     help="split the room into slabs along i (torchrun ranks, or --slabs on one GPU)")
     ap.add_argument("--slabs", type=int, default=2)
+    ap.add_argument("--peer", action="store_true",
+                    help="with --decompose: the step writes the neighbours' ghost planes itself")
     ap.add_argument("--serve-requests", type=int, default=256)
     ap.add_argument("--serve-load", type=float, default=1.5,
                     help="offered load as a multiple of the sequential plain capacity")
@@ -572,9 +574,9 @@ def slab_arm(args):
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
-        run = distributed_room(room, rank, world)
+        run = distributed_room(room, rank, world, peer_memory=args.peer)
     else:
-        run = local_room(room, args.slabs)
+        run = local_room(room, args.slabs, peer_stores=args.peer)
     run.step(args.warmup)
     if world > 1:
         dist.barrier()
@@ -598,7 +600,9 @@ def slab_arm(args):
                 "dtype": "f32", "data": "synthetic",
                 "config": {"workload": room.name, "cells": room.cells,
                            "parallelism": f"slab{world if world > 1 else args.slabs}",
-                           "exchange": "NCCL send/recv" if world > 1 else "in-process plane copies",
+                           "exchange": ("fused peer stores + " + ("NCCL one-word all-reduce barrier" if world > 1
+                                                                   else "stream order")) if args.peer else
+                                       ("NCCL send/recv" if world > 1 else "in-process plane copies"),
                            "kernel": ("fused single-pass kernel on slabs, one exchange per step" if run.fused
                                       else "two-pass slab kernels, two exchanges per step")},
                 "gpu_launches": launches, "traces_finite": bool(np.isfinite(tr).all())}

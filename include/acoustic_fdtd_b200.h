@@ -393,6 +393,14 @@ FDTD_B200_API int fdtd_b200_slab_set_receivers(FdtdB200Slab* h, int n_rec, const
 FDTD_B200_API int fdtd_b200_slab_deposit(FdtdB200Slab* h, int n);
 /* Fused single-pass step of the own planes (flips both current indices). */
 FDTD_B200_API int fdtd_b200_slab_step(FdtdB200Slab* h);
+/* The fused step can also write the neighbours' ghost planes itself (3 planes
+ * of the new P, 2 of the new Vx per side), so that only a barrier separates
+ * the steps: side 0 = left, 1 = right; fields = the neighbour's eight fields
+ * in the same order as fdtd_b200_slab_create's, as pointers writable here
+ * (same device, peer access or an IPC mapping), NULL to clear; [peer_i0,
+ * peer_i1) = its planes.  Neighbours must step in lockstep. */
+FDTD_B200_API int fdtd_b200_slab_set_peer(FdtdB200Slab* h, int side, float* const* fields, int peer_i0,
+                                          int peer_i1);
 FDTD_B200_API int fdtd_b200_slab_velocity(FdtdB200Slab* h);
 FDTD_B200_API int fdtd_b200_slab_pressure(FdtdB200Slab* h);
 FDTD_B200_API int fdtd_b200_slab_record(FdtdB200Slab* h);

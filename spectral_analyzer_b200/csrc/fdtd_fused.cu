@@ -426,7 +426,13 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                     }
                     vnew = vel4_general(cf, pm, p0, p1, p2, vo, aL, aR, fourth ? 15 : 0, okx);
                 }
-                if (f >= i_beg && f < i_end && st_ok) stg4(a.vout[0] + f * PL + own, vnew);
+                if (f >= i_beg && f < i_end && st_ok) {
+                    stg4(a.vout[0] + f * PL + own, vnew);
+#pragma unroll
+                    for (int sd = 0; sd < 2; ++sd)   // the neighbours' ghost faces
+                        if (a.pr.vx[sd] && f >= a.pr.v_lo[sd] && f < a.pr.v_hi[sd])
+                            stg4(a.pr.vx[sd] + (f + a.pr.dl[sd]) * PL + own, vnew);
+                }
             }
             qx0 = qx1; qx1 = qx2; qx2 = qx3; qx3 = vnew;
         }
@@ -549,7 +555,13 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                         for (int q = 0; q < 4; ++q)
                             if (kb + q >= nz) at(out, q) = 0.0f;
                     }
-                    if (kb < sz) stg4(a.pn + ib + own, out);
+                    if (kb < sz) {
+                        stg4(a.pn + ib + own, out);
+#pragma unroll
+                        for (int sd = 0; sd < 2; ++sd)   // the neighbours' ghost planes
+                            if (a.pr.pn[sd] && i >= a.pr.p_lo[sd] && i < a.pr.p_hi[sd])
+                                stg4(a.pr.pn[sd] + (i + a.pr.dl[sd]) * PL + own, out);
+                    }
                 }
             }
         }
@@ -654,6 +666,7 @@ __global__ void __launch_bounds__(C::NT, 2) k_fused_batch(BatchMember* __restric
         }
         a.status = status;
         a.xs = XSpan{0, 0, 0, 0};
+        a.pr = XPeers{};
         const int local = item - m->items_begin;
         if (!fused_tile<C>(a, &m->maps[par][0], &m->maps[par][1], &m->maps[par][2], &m->maps[par][3],
                            local % m->tiles, local / m->tiles, m->seg_len, m->tiles_k, smem, sbase,

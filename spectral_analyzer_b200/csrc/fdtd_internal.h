@@ -146,6 +146,19 @@ struct XSpan {
     int n_own;   // own planes
 };
 
+// Peer slabs' ghost planes written by the step itself (a slab of a split
+// room): side 0 = the left neighbour, 1 = the right one.  pn/vx are the
+// neighbour's next P buffer and next Vx set (null: no neighbour or no peer
+// stores); local plane l of this slab is plane l + dl of the neighbour;
+// planes [p_lo, p_hi) of the new P and faces [v_lo, v_hi) of the new Vx go
+// there.  Memory may be another GPU's (peer access or IPC mapping).
+struct XPeers {
+    float* pn[2];
+    float* vx[2];
+    int dl[2];
+    int p_lo[2], p_hi[2], v_lo[2], v_hi[2];
+};
+
 struct FusedArgs {
     Grid g;
     Coef cf;
@@ -156,6 +169,7 @@ struct FusedArgs {
     float* vout[3];        // V^{n+1/2}
     unsigned* status;      // kStatusTimeout is set if a load wait runs out
     XSpan xs;              // zero: whole room
+    XPeers pr;             // zero: no peer stores
 };
 struct FusedCache;         // host-side TMA descriptors of a handle's fields
 FusedCache* fused_cache_create();

@@ -188,6 +188,10 @@ struct FdtdB200Slab {
     int cap = 0, rows = 0;
     unsigned long long* d_bad = nullptr;
     unsigned* d_status = nullptr;   // timeout word of the fused step
+    // neighbours whose ghost planes the fused step writes directly (side 0 left, 1 right)
+    float* peer_p[2][2] = {};       // [side][buffer]
+    float* peer_vx[2][2] = {};      // [side][velocity set]
+    int peer_dl[2] = {0, 0};
     long long launches = 0;
 };
 
@@ -398,6 +402,32 @@ int fdtd_b200_slab_pressure(FdtdB200Slab* h)
     return FDTD_OK;
 }
 
+// Neighbour fields for the fused step's direct ghost stores.  fields: the
+// neighbour's eight fields {P0, P1, Vx0, Vy0, Vz0, Vx1, Vy1, Vz1} as pointers
+// this process can write (the same device, peer access, or an IPC mapping);
+// NULL clears the side.  The neighbour must step in lockstep (same buffer
+// parities) and own the planes [peer_i0, peer_i1) next to this slab.
+int fdtd_b200_slab_set_peer(FdtdB200Slab* h, int side, float* const* fields, int peer_i0, int peer_i1)
+{
+    if (!h) return FDTD_ERR_NULL;
+    if (side != 0 && side != 1) return FDTD_ERR_ARG;
+    if (!fields) {
+        h->peer_p[side][0] = h->peer_p[side][1] = nullptr;
+        h->peer_vx[side][0] = h->peer_vx[side][1] = nullptr;
+        return FDTD_OK;
+    }
+    if (peer_i1 - peer_i0 < 3 || (side == 0 && peer_i1 != h->i0) || (side == 1 && peer_i0 != h->i1))
+        return FDTD_ERR_ARG;
+    for (int q = 0; q < 8; ++q)
+        if (!fields[q]) return FDTD_ERR_NULL;
+    h->peer_p[side][0] = fields[0];
+    h->peer_p[side][1] = fields[1];
+    h->peer_vx[side][0] = fields[2];
+    h->peer_vx[side][1] = fields[5];
+    h->peer_dl[side] = h->i0 - peer_i0;   // local plane l here is plane l + dl there
+    return FDTD_OK;
+}
+
 // One fused step of the own planes: P[cur] -> P[cur^1], V set cv -> cv^1.
 int fdtd_b200_slab_step(FdtdB200Slab* h)
 {
@@ -414,6 +444,20 @@ int fdtd_b200_slab_step(FdtdB200Slab* h)
     FusedArgs a{h->s.g, h->cf, h->tb, h->P[h->cur], h->P[h->cur ^ 1], {vi[0], vi[1], vi[2]},
                 {vo[0], vo[1], vo[2]}, h->d_status,
                 XSpan{h->s.x0, h->s.nxg, h->s.own_lo, h->i1 - h->i0}};
+    const int own = h->i1 - h->i0;
+    for (int sd = 0; sd < 2; ++sd) {
+        if (!h->peer_p[sd][0]) continue;
+        // left neighbour: its ghosts own_L+3 .. own_L+5 (P) and own_L+3, own_L+4 (Vx) are
+        // this slab's planes 3 .. 5 and faces 3, 4; right neighbour: its ghosts 0 .. 2 (P)
+        // and 1, 2 (Vx) are this slab's planes own .. own+2 and faces own+1, own+2
+        a.pr.pn[sd] = h->peer_p[sd][h->cur ^ 1];
+        a.pr.vx[sd] = h->peer_vx[sd][h->cv ^ 1];
+        a.pr.dl[sd] = h->peer_dl[sd];
+        a.pr.p_lo[sd] = sd == 0 ? 3 : own;
+        a.pr.p_hi[sd] = sd == 0 ? 6 : own + 3;
+        a.pr.v_lo[sd] = sd == 0 ? 3 : own + 1;
+        a.pr.v_hi[sd] = sd == 0 ? 5 : own + 3;
+    }
     SCK(launch_fused_step(a, h->fcache, h->stream));
     ++h->launches;
     h->cur ^= 1;

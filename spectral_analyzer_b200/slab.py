@@ -24,7 +24,12 @@ single-GPU engine's bit for bit.
 Backends: ``EngineSlab`` (the CUDA slab kernels, fields as torch CUDA
 tensors).  Exchanges: ``DistExchange`` (torch.distributed point-to-point:
 NCCL over NVLink between GPUs, or gloo between CPU processes) and
-``LocalExchange`` (several slabs in one process, plane copies).
+``LocalExchange`` (several slabs in one process, plane copies).  With peer
+stores the fused step itself writes the neighbours' ghost planes (their next
+buffers) through pointers to their fields, so no exchange runs at all:
+``PeerStores`` for slabs in one process, ``PeerDistExchange`` across
+processes (fields shared through CUDA IPC; between steps only a barrier —
+a stream-ordered NCCL all-reduce of one word, or a host barrier).
 """
 from __future__ import annotations
 
@@ -128,6 +133,16 @@ class EngineSlab:
     def step(self):
         self._check(self._lib.fdtd_b200_slab_step(self._h), "slab_step")
 
+    def set_peer(self, side: int, fields, i0: int, i1: int):
+        """Let the fused step write the neighbour's ghost planes: fields = its
+        eight tensors (or None to clear), [i0, i1) = its planes."""
+        if fields is None:
+            self._check(self._lib.fdtd_b200_slab_set_peer(self._h, int(side), None, 0, 0), "slab_set_peer")
+            return
+        ptrs = (C.c_void_p * 8)(*[t.data_ptr() for t in fields])
+        self._check(self._lib.fdtd_b200_slab_set_peer(self._h, int(side), C.cast(ptrs, C.POINTER(C.c_void_p)),
+                                                      int(i0), int(i1)), "slab_set_peer")
+
     def velocity(self):
         self._check(self._lib.fdtd_b200_slab_velocity(self._h), "slab_velocity")
 
@@ -179,6 +194,20 @@ class LocalExchange:
 
     def gather(self, obj) -> list:
         return [obj]
+
+
+class PeerStores(LocalExchange):
+    """Slabs in one process whose fused steps write each other's ghost planes:
+    nothing to exchange (the kernels run in order on one stream)."""
+
+    def __init__(self, slabs):
+        super().__init__(slabs)
+        for a, b in zip(self.slabs[:-1], self.slabs[1:]):
+            a.set_peer(1, b.fields, b.i0, b.i1)
+            b.set_peer(0, a.fields, a.i0, a.i1)
+
+    def exchange(self, *names: str):
+        pass
 
 
 class DistExchange:
@@ -276,20 +305,66 @@ class SlabRunner:
         return np.concatenate([p for _, p in gathered], axis=0)
 
 
-def local_room(room: Room, n_slabs: int, device=None, fused: bool = True) -> SlabRunner:
-    """All slabs of a room in this process on one GPU (tests, single-GPU runs)."""
+class PeerDistExchange(DistExchange):
+    """This rank's fused step writes its neighbours' ghost planes directly
+    (their fields mapped here through CUDA IPC); a step then ends with a
+    barrier instead of an exchange: a stream-ordered NCCL all-reduce of one
+    word (every rank's step has finished, so its stores have landed), or,
+    without NCCL, a stream synchronisation and a host barrier."""
+
+    def __init__(self, slab, rank: int, world: int, group=None):
+        import torch
+        import torch.distributed as dist
+        from torch.multiprocessing.reductions import reduce_tensor
+        super().__init__(slab, rank, world, group)
+        mine = (rank, slab.i0, slab.i1, [reduce_tensor(t) for t in slab.fields])
+        infos = self.gather(mine)
+        self._peers = []                     # keeps the IPC mappings alive
+        for side, other in ((0, rank - 1), (1, rank + 1)):
+            if 0 <= other < world:
+                r, i0, i1, handles = infos[other]
+                tensors = [fn(*args) for fn, args in handles]
+                self._peers.append(tensors)
+                slab.set_peer(side, tensors, i0, i1)
+        self._nccl = dist.get_backend(group) == "nccl"
+        self._token = torch.zeros(1, dtype=torch.int32, device=slab.device)
+
+    def exchange(self, *names: str):
+        import torch
+        import torch.distributed as dist
+        if self._nccl:
+            dist.all_reduce(self._token, group=self.group)
+        else:
+            torch.cuda.current_stream(self.slab.device).synchronize()
+            dist.barrier(group=self.group)
+
+
+def local_room(room: Room, n_slabs: int, device=None, fused: bool = True, peer_stores: bool = False) -> SlabRunner:
+    """All slabs of a room in this process on one GPU (tests, single-GPU runs);
+    peer_stores: the fused steps write each other's ghost planes directly."""
     ranges = partition(room.nx, n_slabs)
     owners = receiver_owner(room, ranges)
     slabs = [EngineSlab(room, a, b, [q for q, o in enumerate(owners) if o == r], device, fused)
              for r, (a, b) in enumerate(ranges)]
+    if peer_stores:
+        if not fused:
+            raise ValueError("peer stores come with the fused step")
+        return SlabRunner(slabs, PeerStores(slabs))
     return SlabRunner(slabs, LocalExchange(slabs))
 
 
 def distributed_room(room: Room, rank: int, world: int, group=None, device=None,
-                     fused: bool = True) -> SlabRunner:
-    """This rank's slab of a room split over `world` ranks (torch.distributed initialised)."""
+                     fused: bool = True, peer_memory: bool = False) -> SlabRunner:
+    """This rank's slab of a room split over `world` ranks (torch.distributed
+    initialised); peer_memory: the fused step writes the neighbours' ghost
+    planes through CUDA IPC mappings of their fields and steps end with a
+    barrier (the ranks' GPUs must reach each other's memory)."""
     ranges = partition(room.nx, world)
     owners = receiver_owner(room, ranges)
     a, b = ranges[rank]
     slab = EngineSlab(room, a, b, [q for q, o in enumerate(owners) if o == rank], device, fused)
+    if peer_memory:
+        if not fused:
+            raise ValueError("peer stores come with the fused step")
+        return SlabRunner([slab], PeerDistExchange(slab, rank, world, group))
     return SlabRunner([slab], DistExchange(slab, rank, world, group))

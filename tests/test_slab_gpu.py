@@ -32,13 +32,14 @@ def edge_room():
                 (0.3, 0.9, 0.5, 1.0, 0.2, 0.7), "ricker", n_pml=6)
 
 
-@pytest.mark.parametrize("fused", [True, False])
+@pytest.mark.parametrize("fused,peer", [(True, False), (False, False), (True, True)])
 @pytest.mark.parametrize("n_slabs", [1, 2, 3, 5])
-def test_slabs_equal_whole_room(cuda, n_slabs, fused):
+def test_slabs_equal_whole_room(cuda, n_slabs, fused, peer):
+    """peer: the fused steps write each other's ghost planes, no exchange."""
     from spectral_analyzer_b200.slab import local_room
     room = edge_room()
     tr, P = whole(room)
-    run = local_room(room, n_slabs, fused=fused)
+    run = local_room(room, n_slabs, fused=fused, peer_stores=peer)
     assert run.fused == fused
     run.step(room.n_steps)
     got = run.traces(len(room.receivers))
