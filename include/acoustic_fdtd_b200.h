@@ -134,6 +134,13 @@ FDTD_B200_API int fdtd_reset(AcousticFDTDState* st);
 
 /* acoustic_fdtd.h:359-363, :372-376. */
 FDTD_B200_API int fdtd_get_pressure_field(const AcousticFDTDState* st, float* out, int out_len);
+/* One pressure plane, as acoustic_fdtd_bridge.py:737-757 (get_volume_slice)
+ * returns it, without copying the whole field: axis 0 -> (Ny, Nz) at i = idx,
+ * 1 -> (Nx, Nz) at j = idx, 2 -> (Nx, Ny) at k = idx; idx < 0 is the mid
+ * plane, idx past the end the last plane.  out_len must equal the plane's
+ * size (FDTD_ERR_DIM); axis outside 0..2 is FDTD_ERR_ARG. */
+FDTD_B200_API int fdtd_b200_get_volume_slice(const AcousticFDTDState* st, int axis, int idx, float* out,
+                                             int out_len);
 FDTD_B200_API int fdtd_get_plate_displacement(const AcousticFDTDState* st, float* out,
                                               int out_len);
 
@@ -222,6 +229,15 @@ FDTD_B200_API int fdtd_b200_synchronize(AcousticFDTDState* st);
  * the scene has walls, fractions or an active plate). */
 FDTD_B200_API int fdtd_b200_set_kernel(AcousticFDTDState* st, int mode);
 FDTD_B200_API int fdtd_b200_get_kernel(const AcousticFDTDState* st);
+
+/* Failure-path hook for tests of the fused step's bounded waits (no reference
+ * counterpart).  From the next fused step on, the TMA load of pressure plane
+ * `plane` (0 .. Nx-1) is armed on its mbarrier but never issued, so every CTA
+ * that needs it gives up after `wait_us` microseconds (0: the normal bound of
+ * 2 s), records a timeout status and exits, leaving that step incomplete.
+ * fdtd_b200_synchronize then returns FDTD_ERR_CUDA ("load wait timed out")
+ * until fdtd_reset; the CUDA context stays usable.  plane -1 turns it off. */
+FDTD_B200_API int fdtd_b200_debug_hold_load(AcousticFDTDState* st, int plane, int wait_us);
 
 /* Device pointers of the current fields: out5 = {P (current), P (next), Vx, Vy, Vz}. */
 FDTD_B200_API int fdtd_b200_device_fields(const AcousticFDTDState* st, void** out5);

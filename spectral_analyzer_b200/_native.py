@@ -40,6 +40,7 @@ SIGNATURES = {
     "fdtd_get_dt": (f32, [vp]),
     "fdtd_reset": (i32, [vp]),
     "fdtd_get_pressure_field": (i32, [vp, P_f32, i32]),
+    "fdtd_b200_get_volume_slice": (i32, [vp, i32, i32, P_f32, i32]),
     "fdtd_get_plate_displacement": (i32, [vp, P_f32, i32]),
     "fdtd_sample_plate_displacement_batch": (i32, [vp, i32, P_i32, P_f32, P_f32]),
     "fdtd_sample_pressure": (i32, [vp, i32, P_f32, P_f32]),
@@ -63,6 +64,7 @@ SIGNATURES = {
     "fdtd_b200_step_async": (i32, [vp, i32]),
     "fdtd_b200_synchronize": (i32, [vp]),
     "fdtd_b200_set_kernel": (i32, [vp, i32]),
+    "fdtd_b200_debug_hold_load": (i32, [vp, i32, i32]),
     "fdtd_b200_get_kernel": (i32, [vp]),
     "fdtd_b200_device_fields": (i32, [vp, C.POINTER(vp)]),
     "fdtd_b200_profile": (i32, [vp, i32]),

@@ -115,6 +115,7 @@ struct AcousticFDTDState {
     float* d_w[3] = {nullptr, nullptr, nullptr};
     int wi_cur = 0, wi_prev = 1, wi_tmp = 2;
     float* d_ext = nullptr;
+    float* d_slice = nullptr;        // fdtd_b200_get_volume_slice staging, largest plane
     float* h_ext = nullptr;          // pinned, N_plate: forces pending for the next step
     bool ext_pending = false;
     bool dev_ext_nonzero = false;
@@ -128,6 +129,7 @@ struct AcousticFDTDState {
     int ps_n = 0;
     int ps_cell = -1;
     int ps_done_step = -1;           // step whose source sample is already in P
+    int rec_pending = -1;            // trace slot the next fused step (or flush_record) records
 
     // receivers
     int n_rec = 0;
@@ -143,6 +145,8 @@ struct AcousticFDTDState {
     int stab_phase = 0;
 
     int kernel_mode = 0;
+    int hold_plane = kNoPlane;       // fdtd_b200_debug_hold_load
+    unsigned wait_us = kWaitUs;
     FusedCache* fcache = nullptr;    // TMA descriptors of the fields (fused step)
 
     long long launches = 0;          // kernels launched by this handle
@@ -494,17 +498,42 @@ int alloc_second_velocity_set(AcousticFDTDState* st)
     return FDTD_OK;
 }
 
+// Records the receivers of the current pressure into the pending trace slot
+// (a record a fused step left for the next one to take).
+int flush_record(AcousticFDTDState* st)
+{
+    if (st->rec_pending < 0) return FDTD_OK;
+    const int slot = st->rec_pending;
+    st->rec_pending = -1;
+    CK(launch_wsum(st->P(), st->d_rec_idx, st->d_rec_w, st->n_rec, 8, 0,
+                   st->d_trace + (size_t)slot * st->n_rec, st->stream));
+    ++st->launches;
+    return FDTD_OK;
+}
+
 // One time step (acoustic_fdtd.cpp:1272-1290 loop body) plus the engine's
 // point-source deposit before it and receiver record after it.
 // sync_check: stop and return FDTD_ERR_UNSTABLE at a failed check (fdtd_step);
 // otherwise failures are latched on the device (fdtd_b200_step_async).
-int one_step(AcousticFDTDState* st, bool sync_check)
+// defer_record: a fused step leaves its receiver record pending, to be taken
+// by the next fused step's kernel from its input pressure; the caller ends
+// its run of steps with flush_record.  On the fused path the point-source
+// deposit of an open source cell is applied inside the step kernel too.
+int one_step(AcousticFDTDState* st, bool sync_check, bool defer_record = false)
 {
     cudaStream_t s = st->stream;
+    const bool fused = use_fused(st);
+    if (!fused) {
+        if (int rc0 = flush_record(st)) return rc0;
+    }
     // point source: deposit s[n] before step n (applies before the plate reads P)
+    bool fuse_deposit = false;
     if (st->ps_n > 0 && st->step_count < st->ps_n && st->ps.n > 0 && st->ps_done_step != st->step_count) {
-        CK(launch_deposit(st->ps, st->d_ps_sig, st->step_count, 0.0f, st->P(), s));
-        ++st->launches;
+        fuse_deposit = fused && st->ps.n == 1 && st->ps.divisor == 0;
+        if (!fuse_deposit) {
+            CK(launch_deposit(st->ps, st->d_ps_sig, st->step_count, 0.0f, st->P(), s));
+            ++st->launches;
+        }
         st->ps_done_step = st->step_count;
     }
 
@@ -556,7 +585,7 @@ int one_step(AcousticFDTDState* st, bool sync_check)
     cudaEvent_t e1;
     int rc = prof_begin(st, &e1);
     if (rc) return rc;
-    if (use_fused(st)) {
+    if (fused) {
         if (!st->v[st->cv ^ 1][0]) {
             int rc2 = alloc_second_velocity_set(st);
             if (rc2) return rc2;
@@ -566,6 +595,23 @@ int one_step(AcousticFDTDState* st, bool sync_check)
                     {st->V(0), st->V(1), st->V(2)},
                     {st->v[st->cv ^ 1][0], st->v[st->cv ^ 1][1], st->v[st->cv ^ 1][2]},
                     st->d_status};
+        a.hold_plane = st->hold_plane;
+        a.wait_us = st->wait_us;
+        if (fuse_deposit) {
+            const long long c = st->ps.idx[0], t = c / st->g.sz;
+            a.dep_sig = st->d_ps_sig;
+            a.dep_step = st->step_count;
+            a.dep_i = (int)(t / st->Ny);
+            a.dep_j = (int)(t % st->Ny);
+            a.dep_k = (int)(c % st->g.sz);
+        }
+        if (st->rec_pending >= 0) {
+            a.rec_idx = st->d_rec_idx;
+            a.rec_w = st->d_rec_w;
+            a.rec_out = st->d_trace + (size_t)st->rec_pending * st->n_rec;
+            a.n_rec = st->n_rec;
+            st->rec_pending = -1;
+        }
         CK(launch_fused_step(a, st->fcache, s));
         ++st->launches;
         st->cv ^= 1;
@@ -589,10 +635,14 @@ int one_step(AcousticFDTDState* st, bool sync_check)
 
     // receivers
     if (st->n_rec > 0 && st->trace_len < st->trace_cap) {
-        CK(launch_wsum(st->P(), st->d_rec_idx, st->d_rec_w, st->n_rec, 8, 0,
-                       st->d_trace + (size_t)st->trace_len * st->n_rec, s));
+        if (fused && defer_record) {
+            st->rec_pending = st->trace_len;
+        } else {
+            CK(launch_wsum(st->P(), st->d_rec_idx, st->d_rec_w, st->n_rec, 8, 0,
+                           st->d_trace + (size_t)st->trace_len * st->n_rec, s));
+            ++st->launches;
+        }
         ++st->trace_len;
-        ++st->launches;
     }
 
     // stability check every 256 steps (acoustic_fdtd.cpp:1284-1287)
@@ -634,7 +684,7 @@ void free_state(AcousticFDTDState* st)
     cudaFree(st->d_solid);
     for (int c = 0; c < 3; ++c) { cudaFree(st->d_frac[c]); cudaFree(st->d_w[c]); }
     cudaFree(st->d_act); cudaFree(st->d_nb13); cudaFree(st->d_above); cudaFree(st->d_below);
-    cudaFree(st->d_vzb); cudaFree(st->d_vza); cudaFree(st->d_ext);
+    cudaFree(st->d_vzb); cudaFree(st->d_vza); cudaFree(st->d_ext); cudaFree(st->d_slice);
     cudaFreeHost(st->h_ext);
     cudaFree(st->d_ps_sig);
     cudaFree(st->d_rec_idx); cudaFree(st->d_rec_w); cudaFree(st->d_trace);
@@ -1007,11 +1057,10 @@ int fdtd_step(AcousticFDTDState* st, int n_steps)
     if (!st) return FDTD_ERR_NULL;
     if (n_steps <= 0) return FDTD_OK;
     if (dev_guard(st)) return FDTD_ERR_CUDA;
-    for (int s = 0; s < n_steps; ++s) {
-        int rc = one_step(st, true);
-        if (rc) return rc;
-    }
-    return FDTD_OK;
+    int rc = FDTD_OK;
+    for (int s = 0; s < n_steps && rc == FDTD_OK; ++s) rc = one_step(st, true, true);
+    const int rc_rec = flush_record(st);
+    return rc != FDTD_OK ? rc : rc_rec;
 }
 
 int fdtd_get_step_count(const AcousticFDTDState* st) { return st ? st->step_count : 0; }
@@ -1026,13 +1075,38 @@ int fdtd_reset(AcousticFDTDState* st)
         if (f) CK(cudaMemsetAsync(f, 0, st->field_bytes, st->stream));
     for (int c = 0; c < 3; ++c) CK(cudaMemsetAsync(st->d_w[c], 0, sizeof(float) * st->N_plate, st->stream));
     CK(cudaMemsetAsync(st->d_ext, 0, sizeof(float) * st->N_plate, st->stream));
+    // a latched fused-step timeout or instability ends with the state it spoiled
+    CK(cudaMemsetAsync(st->d_status, 0xFF, kStatusWords * sizeof(unsigned), st->stream));
     CK(cudaStreamSynchronize(st->stream));
+    for (int w = 0; w < kStatusWords; ++w) st->h_status[w] = 0xFFFFFFFFu;
     memset(st->h_ext, 0, sizeof(float) * st->N_plate);
     st->ext_pending = false;
     st->dev_ext_nonzero = false;
     st->step_count = 0;
     st->trace_len = 0;
     st->ps_done_step = -1;
+    return FDTD_OK;
+}
+
+int fdtd_b200_get_volume_slice(const AcousticFDTDState* cst, int axis, int idx, float* out, int out_len)
+{   // acoustic_fdtd_bridge.py:737-757 without the full-field copy
+    AcousticFDTDState* st = const_cast<AcousticFDTDState*>(cst);
+    if (!st || !out) return FDTD_ERR_NULL;
+    if (axis < 0 || axis > 2) return FDTD_ERR_ARG;
+    const int dims[3] = {st->Nx, st->Ny, st->Nz};
+    const int na = axis == 0 ? st->Ny : st->Nx, nb = axis == 2 ? st->Ny : st->Nz;
+    if ((long long)out_len != (long long)na * nb) return FDTD_ERR_DIM;
+    if (idx < 0) idx = dims[axis] / 2;
+    idx = std::min(idx, dims[axis] - 1);
+    if (dev_guard(st)) return FDTD_ERR_CUDA;
+    if (!st->d_slice) {
+        const size_t most = (size_t)std::max({(long long)st->Ny * st->Nz, (long long)st->Nx * st->Nz,
+                                              (long long)st->Nx * st->Ny});
+        CK(cudaMalloc(&st->d_slice, most * sizeof(float)));
+    }
+    CK(launch_slice(st->P(), st->g, axis, idx, st->d_slice, na, nb, st->stream));
+    CK(cudaMemcpyAsync(out, st->d_slice, sizeof(float) * (size_t)out_len, cudaMemcpyDeviceToHost, st->stream));
+    CK(cudaStreamSynchronize(st->stream));
     return FDTD_OK;
 }
 
@@ -1259,11 +1333,10 @@ int fdtd_b200_step_async(AcousticFDTDState* st, int n_steps)
     if (!st) return FDTD_ERR_NULL;
     if (n_steps <= 0) return FDTD_OK;
     if (dev_guard(st)) return FDTD_ERR_CUDA;
-    for (int s = 0; s < n_steps; ++s) {
-        int rc = one_step(st, false);
-        if (rc) return rc;
-    }
-    return FDTD_OK;
+    int rc = FDTD_OK;
+    for (int s = 0; s < n_steps && rc == FDTD_OK; ++s) rc = one_step(st, false, true);
+    const int rc_rec = flush_record(st);
+    return rc != FDTD_OK ? rc : rc_rec;
 }
 
 int fdtd_b200_synchronize(AcousticFDTDState* st)
@@ -1280,6 +1353,15 @@ int fdtd_b200_synchronize(AcousticFDTDState* st)
         CK(cudaStreamSynchronize(st->stream));
         return FDTD_ERR_UNSTABLE;
     }
+    return FDTD_OK;
+}
+
+int fdtd_b200_debug_hold_load(AcousticFDTDState* st, int plane, int wait_us)
+{
+    if (!st) return FDTD_ERR_NULL;
+    if (plane < -1 || plane >= st->Nx || wait_us < 0 || (unsigned)wait_us > kWaitUs) return FDTD_ERR_ARG;
+    st->hold_plane = plane < 0 ? kNoPlane : plane;
+    st->wait_us = wait_us > 0 ? (unsigned)wait_us : kWaitUs;
     return FDTD_OK;
 }
 
@@ -1489,7 +1571,8 @@ int batch_pull(FdtdB200Batch* b, int* steps_out, int* status_out)
         st->trace_len = std::min(m.trace0 + done, m.trace_cap);
         const int n_chk = m.step / kCheckPeriod - m.step0 / kCheckPeriod;
         st->stab_phase = (m.phase0 + n_chk) % kCheckStride;
-        if (m.step < m.limit && m.step < m.ps_n) st->ps_done_step = m.step;
+        // the epilogue deposited step m.step's sample unless the member stopped unstable
+        if (m.step < m.limit && m.step < m.ps_n && m.unstable == 0xFFFFFFFFu) st->ps_done_step = m.step;
         if (steps_out) steps_out[q] = m.step;
         if (status_out) status_out[q] = (m.unstable != 0xFFFFFFFFu) ? FDTD_ERR_UNSTABLE : FDTD_OK;
     }

@@ -97,8 +97,6 @@ struct Cfg {
     static_assert(TJ % RW == 0 && HW * 32 <= NT, "whole warps of rows; halo warps exist");
 };
 
-constexpr int kWaitSpins = 1 << 21;   // bound on mbarrier polls (each poll may block briefly)
-
 __device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
 
 __device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
@@ -122,11 +120,24 @@ __device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity)
     return ok != 0;
 }
 
-// Bounded wait for the phase with the given parity; false when the bound ran out.
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity)
+__device__ __forceinline__ unsigned long long global_ns()
 {
-    for (int it = 0; it < kWaitSpins; ++it)
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+    return t;
+}
+
+// Bounded wait for the phase with the given parity: polls until it completes,
+// limit_us of wall time has passed, or kWaitPolls polls were made (whichever
+// comes first); false when a bound ran out.  The first poll reads no clock.
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned limit_us)
+{
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = global_ns(), limit = 1000ull * limit_us;
+    for (int it = 0; it < kWaitPolls; ++it) {
         if (mbar_try(bar, parity)) return true;
+        if (global_ns() - t0 > limit) return false;
+    }
     return false;
 }
 
@@ -302,7 +313,8 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
         const unsigned pb = bar0 + 8u * ps;
         mbar_expect_tx(pb, C::P_BYTES);
-        tma_load3(sbase + 4u * (C::RING0 + ps * C::P_STAGE), tmP, k0 - 4, j0 - 3, u, pb);
+        if (u != a.hold_plane)
+            tma_load3(sbase + 4u * (C::RING0 + ps * C::P_STAGE), tmP, k0 - 4, j0 - 3, u, pb);
         const int f = u - 2, io = u - 3, fg = f + xg0;
         const bool vx = (u >= i_beg && fg >= 0 && fg <= nxg - 2);
         const bool vyz = (io >= i_beg && io < i_end);
@@ -389,8 +401,17 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
         // timeout is made by the whole CTA (the barrier below is also the one that
         // separates the previous iteration's reads from this iteration's writes)
         const int ps = pslot[3], vsg = vslot[0];
-        const bool ok = mbar_wait(bar0 + 8u * ps, (pph >> ps) & 1u) &&
-                        mbar_wait(bar0 + 8u * (C::RING + vsg), (vph >> vsg) & 1u);
+        const bool ok = mbar_wait(bar0 + 8u * ps, (pph >> ps) & 1u, a.wait_us) &&
+                        mbar_wait(bar0 + 8u * (C::RING + vsg), (vph >> vsg) & 1u, a.wait_us);
+        // the source deposit, on the arriving plane's shared copy before anyone reads it
+        if (a.dep_sig && u == a.dep_i && tid == 0 && ok) {
+            const int dj = a.dep_j - (j0 - 3), dk = a.dep_k - (k0 - 4);
+            const float amp = a.dep_sig[a.dep_step];
+            if (dj >= 0 && dj < C::PR && dk >= 0 && dk < C::PC && amp != 0.0f) {
+                float* c = smem + C::RING0 + ps * C::P_STAGE + dj * C::PC + dk;
+                *c = fadd(*c, amp);
+            }
+        }
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicMin(a.status + kStatusTimeout, blockIdx.x + gridDim.x * blockIdx.y);
             u_fail = u;
@@ -593,8 +614,8 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
         if (tid == 0) {
             for (int q = 0; q < C::D && u_fail + q <= u1; ++q) {
                 const int ps = pslot[3 + q], vsg = vslot[q];
-                mbar_wait(bar0 + 8u * ps, (pph >> ps) & 1u);
-                mbar_wait(bar0 + 8u * (C::RING + vsg), (vph >> vsg) & 1u);
+                mbar_wait(bar0 + 8u * ps, (pph >> ps) & 1u, a.wait_us);
+                mbar_wait(bar0 + 8u * (C::RING + vsg), (vph >> vsg) & 1u, a.wait_us);
             }
         }
         __syncthreads();
@@ -612,6 +633,11 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
                                                       const __grid_constant__ CUtensorMap tmZ,
                                                       int seg_len, int tiles_k)
 {
+    if (a.n_rec > 0) {   // the previous step's receivers, from this step's input P
+        const int nblk = gridDim.x * gridDim.y, b = blockIdx.x + gridDim.x * blockIdx.y;
+        for (int r = b + nblk * (int)threadIdx.x; r < a.n_rec; r += nblk * C::NT)
+            a.rec_out[r] = sample8(a.p, a.rec_idx + 8 * r, a.rec_w + 8 * r);
+    }
     if ((int)blockIdx.y * seg_len >= (a.xs.nxg > 0 ? a.xs.n_own : a.g.nx)) return;
     float* smem;
     const unsigned sbase = smem_base_u32<C>(&smem);
@@ -652,7 +678,7 @@ __global__ void __launch_bounds__(C::NT, 2) k_fused_batch(BatchMember* __restric
         if (item >= total_items) break;
         const BatchMember* m = mem + item_member[item];
         const int step = m->step;
-        if (step >= m->limit) continue;
+        if (step >= m->limit || m->unstable != 0xFFFFFFFFu) continue;   // done, or stopped unstable
         const int par = (step - m->step0) & 1;
         FusedArgs a;
         a.g = m->g;
@@ -678,14 +704,17 @@ __global__ void __launch_bounds__(C::NT, 2) k_fused_batch(BatchMember* __restric
 // After a batched step, per member below its limit: record the receivers from
 // the new pressure, advance the step counter, run the 256-step check, then
 // deposit the next step's source sample (the order of the single-room path:
-// record after step n, deposit before step n+1).  One block per member.
+// record after step n, deposit before step n+1).  One block per member.  A
+// member whose check fails stops at that step without the next deposit, the
+// state a single room is left in when its step returns UNSTABLE; the batch
+// steps it no further until its set is rebuilt.
 __global__ void k_batch_epilogue(BatchMember* __restrict__ mem, const BatchHeader* __restrict__ hdr)
 {
     const int r = blockIdx.x;
     if (r >= hdr->n_members) return;
     BatchMember* m = mem + r;
     const int s = m->step;
-    if (s >= m->limit) return;
+    if (s >= m->limit || m->unstable != 0xFFFFFFFFu) return;
     const int s1 = s + 1;
     float* P = m->p[(s1 - m->step0) & 1];
     const int slot = m->trace0 + (s - m->step0);
@@ -704,9 +733,10 @@ __global__ void k_batch_epilogue(BatchMember* __restrict__ mem, const BatchHeade
             if (!isfinite(v) || v > 2e3f || v < -2e3f) atomicCAS(&m->unstable, 0xFFFFFFFFu, (unsigned)s1);
         }
     }
-    __syncthreads();   // receivers have read P before the deposit below changes it
+    __syncthreads();   // receivers have read P and the check's flags are set
     if (threadIdx.x == 0) {
-        if (s1 < m->limit && s1 < m->ps_n) deposit_apply(m->ps, m->ps_sig[s1], P);
+        const bool stopped = *(volatile unsigned*)&m->unstable != 0xFFFFFFFFu;
+        if (!stopped && s1 < m->limit && s1 < m->ps_n) deposit_apply(m->ps, m->ps_sig[s1], P);
         m->step = s1;
     }
 }

@@ -296,6 +296,20 @@ __global__ void k_zero_gated(float* __restrict__ x, int n, const unsigned* __res
     if (q >= n || gate[kStatusPlate] != 0xFFFFFFFFu) return;
     x[q] = 0.0f;
 }
+
+// One plane of a field across the given axis, rows of the remaining two axes
+// in (i, j, k) order: axis 0 -> (Ny, Nz), 1 -> (Nx, Nz), 2 -> (Nx, Ny).
+__global__ void k_slice(const float* __restrict__ f, Grid g, int axis, int idx, float* __restrict__ out,
+                        int na, int nb)
+{
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= (long long)na * nb) return;
+    const long long a = q / nb, b = q % nb;
+    const long long off = axis == 0 ? ((long long)idx * g.ny + a) * g.sz + b
+                        : axis == 1 ? (a * g.ny + idx) * g.sz + b
+                                    : (a * g.ny + b) * g.sz + idx;
+    out[q] = f[off];
+}
 }  // namespace
 
 cudaError_t launch_velocity_general(const Grid& g, const Coef& cf, const Tables& tb,
@@ -370,6 +384,15 @@ cudaError_t launch_zero_gated(float* x, int n, const unsigned* gate, cudaStream_
 {
     if (n <= 0) return cudaSuccess;
     k_zero_gated<<<(n + 255) / 256, 256, 0, s>>>(x, n, gate);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_slice(const float* f, const Grid& g, int axis, int idx, float* out, int na, int nb,
+                         cudaStream_t s)
+{
+    const long long n = (long long)na * nb;
+    if (n <= 0) return cudaSuccess;
+    k_slice<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(f, g, axis, idx, out, na, nb);
     return cudaGetLastError();
 }
 

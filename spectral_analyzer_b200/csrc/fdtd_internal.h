@@ -133,6 +133,8 @@ cudaError_t launch_check(const Grid& g, const float* p, long long n_cells, int p
 // Kernels given a gate (the handle's status words) do nothing once this step's
 // plate update has recorded a failure in gate[kStatusPlate].
 cudaError_t launch_zero_gated(float* x, int n, const unsigned* gate, cudaStream_t s);
+cudaError_t launch_slice(const float* f, const Grid& g, int axis, int idx, float* out, int na, int nb,
+                         cudaStream_t s);
 
 // ---- fused single-pass step (fdtd_fused.cu) ----
 // A slab of a room split along i: the local grid holds planes of the global
@@ -159,6 +161,13 @@ struct XPeers {
     int p_lo[2], p_hi[2], v_lo[2], v_hi[2];
 };
 
+// Bounds of every mbarrier wait in the fused kernels: wall time (the
+// %globaltimer clock) and, as a backstop, a poll count.
+constexpr unsigned kWaitUs = 2000000u;   // 2 s; a load lands in microseconds
+constexpr int kWaitPolls = 1 << 26;
+// "no plane": plane indices of a march start at -3 (halo planes below i = 0)
+constexpr int kNoPlane = -(1 << 30);
+
 struct FusedArgs {
     Grid g;
     Coef cf;
@@ -170,6 +179,23 @@ struct FusedArgs {
     unsigned* status;      // kStatusTimeout is set if a load wait runs out
     XSpan xs;              // zero: whole room
     XPeers pr;             // zero: no peer stores
+    // Failure-path hook (fdtd_b200_debug_hold_load): the P load of this plane is
+    // armed on its mbarrier but never issued, so its wait runs out after
+    // wait_us microseconds and the kernel takes its timeout exit.
+    int hold_plane = kNoPlane;
+    unsigned wait_us = kWaitUs;
+    // Fused point-source deposit (an open source cell): every CTA that loads
+    // cell (dep_i, dep_j, dep_k) adds dep_sig[dep_step] to its shared-memory
+    // copy of it when the plane arrives, so the step sees P^n plus the deposit
+    // while P^n in HBM is left as it was.  dep_sig null: none.
+    const float* dep_sig = nullptr;
+    int dep_step = 0, dep_i = kNoPlane, dep_j = 0, dep_k = 0;
+    // Fused receiver record of the input pressure (the previous step's
+    // result): rec_out[r] = 8-tap sample of receiver r, spread over the CTAs.
+    const long long* rec_idx = nullptr;
+    const float* rec_w = nullptr;
+    float* rec_out = nullptr;
+    int n_rec = 0;
 };
 struct FusedCache;         // host-side TMA descriptors of a handle's fields
 FusedCache* fused_cache_create();

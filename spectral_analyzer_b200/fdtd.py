@@ -207,6 +207,20 @@ class AcousticFDTD:
     def get_velocity_x(self) -> np.ndarray:
         return self._vel(self._lib.fdtd_get_velocity_x, self._dims[0])
 
+    def get_volume_slice(self, axis: int = 2, idx: int = -1) -> np.ndarray:
+        """2-D pressure plane as the bridge's get_volume_slice returns it
+        (axis 2 -> (Nx, Ny); idx -1 = mid-plane, clamped), gathered on the
+        device so only the plane crosses to the host."""
+        shape = {0: (self.Ny, self.Nz), 1: (self.Nx, self.Nz), 2: (self.Nx, self.Ny)}.get(int(axis))
+        if shape is None:
+            raise ValueError("axis must be 0, 1 or 2")
+        out = np.empty(shape, dtype=np.float32)
+        rc = self._check(self._lib.fdtd_b200_get_volume_slice(self._h, int(axis), int(idx), _pf(out), out.size),
+                         "get_volume_slice")
+        if rc != 0:
+            raise RuntimeError(f"fdtd_b200_get_volume_slice error: {rc}")
+        return out
+
     def get_velocity_y(self) -> np.ndarray:
         return self._vel(self._lib.fdtd_get_velocity_y, self._dims[1])
 
@@ -348,6 +362,12 @@ class AcousticFDTD:
 
     def synchronize(self) -> int:
         return self._check(self._lib.fdtd_b200_synchronize(self._h), "synchronize")
+
+    def debug_hold_load(self, plane: int, wait_us: int = 0):
+        """Test hook: the fused step's load of pressure plane ``plane`` is never
+        issued, so its bounded wait runs out after ``wait_us`` microseconds
+        (0: the normal bound); ``plane=-1`` turns it off."""
+        self._check(self._lib.fdtd_b200_debug_hold_load(self._h, int(plane), int(wait_us)), "debug_hold_load")
 
     def set_kernel(self, mode: str):
         m = {"auto": 0, "two_pass": 1, "fused": 2}[mode]

@@ -12,6 +12,15 @@ through the plain single-room path.
 
 Both compute each room with the same arithmetic, so a room's traces are
 bit-identical alone and in any mix of other rooms.
+
+Failures stay with the request that caused them.  A room whose 256-step check
+fails (FDTD_ERR_UNSTABLE, e.g. a NaN in its source signal) stops on the device
+at that step and leaves with ``error`` set and the traces it recorded; a
+request that does not fit the memory budget even alone, or whose solver cannot
+be allocated, is rejected; ``cancel(rid)`` and a request's ``deadline`` evict
+it at the next chunk boundary.  The other rooms carry on unchanged.  Only an
+engine-level failure (a CUDA error or a timed-out load wait in the batched
+kernel) ends the run.
 """
 from __future__ import annotations
 
@@ -33,20 +42,26 @@ GRID_AXES = tuple(range(32, 257, 16))
 class Request:
     rid: int
     room: Room
-    arrival: float = 0.0        # seconds after the start of the run
+    arrival: float = 0.0                # seconds after the start of the run
+    deadline: Optional[float] = None    # latency budget in seconds (None: none)
 
 
 @dataclass
 class Result:
     rid: int
-    traces: np.ndarray          # (steps, n_rec) float32
+    traces: np.ndarray          # (steps, n_rec) float32; the steps done when error is set
     arrival: float
     start: float
     finish: float
+    error: Optional[str] = None
 
     @property
     def latency(self) -> float:
         return self.finish - self.arrival
+
+    @property
+    def ok(self) -> bool:
+        return self.error is None
 
 
 def room_bytes(room: Room) -> int:
@@ -90,13 +105,17 @@ def percentile(xs: Sequence[float], p: float) -> float:
 
 
 def summarize(results: Sequence[Result], work: float) -> dict:
-    lat = [r.latency for r in results]
+    """Throughput and latency over the completed requests (failed ones counted apart)."""
+    done = [r for r in results if r.ok]
+    lat = [r.latency for r in done]
     t_first = min(r.arrival for r in results)
     t_last = max(r.finish for r in results)
     span = t_last - t_first
-    return {"requests": len(results), "makespan_s": span, "requests_per_s": len(results) / span,
+    return {"requests": len(done), "failed": len(results) - len(done), "makespan_s": span,
+            "requests_per_s": len(done) / span,
             "p50_latency_s": percentile(lat, 50), "p99_latency_s": percentile(lat, 99),
-            "mean_latency_s": float(np.mean(lat)), "gcell_updates_per_s": work / span / 1e9}
+            "mean_latency_s": float(np.mean(lat)) if lat else float("nan"),
+            "gcell_updates_per_s": work / span / 1e9}
 
 
 def request_work(reqs: Sequence[Request]) -> float:
@@ -191,6 +210,12 @@ class BatchServer:
         self.clock = clock
         self.sleep = sleep
         self.log: List[dict] = []
+        self._cancelled: set = set()
+
+    def cancel(self, rid: int) -> None:
+        """Ask for request ``rid`` to be dropped (queued) or evicted (running)
+        at the next scheduling point; safe to call from another thread."""
+        self._cancelled.add(rid)
 
     def run(self, requests: Sequence[Request]) -> List[Result]:
         be = self.backend
@@ -206,39 +231,70 @@ class BatchServer:
         results: List[Result] = []
         t0 = self.clock()
         dirty = False
+
+        def reject(req, now, why):
+            empty = np.zeros((0, len(req.room.receivers)), np.float32)
+            results.append(Result(req.rid, empty, req.arrival, now, now, error=why))
+
+        def late(req, now):
+            return req.deadline is not None and now > req.arrival + req.deadline
+
         while queue or active:
             now = self.clock() - t0
+            # queued requests that were cancelled, ran out of time, or can never fit
+            if queue:
+                keep_q = deque()
+                for req in queue:
+                    if req.rid in self._cancelled:
+                        reject(req, now, "cancelled")
+                    elif late(req, now):
+                        reject(req, now, "deadline exceeded")
+                    elif room_bytes(req.room) > budget:
+                        reject(req, now, "exceeds the memory budget")
+                    else:
+                        keep_q.append(req)
+                queue = keep_q
             while (queue and queue[0].arrival <= now and len(active) < self.max_slots
                    and used + room_bytes(queue[0].room) <= budget):
                 req = queue.popleft()
-                active.append((req, be.make(req.room), now))
+                try:
+                    solver = be.make(req.room)
+                except (RuntimeError, MemoryError) as e:
+                    reject(req, now, f"allocation failed: {e}")
+                    continue
+                active.append((req, solver, now))
                 used += room_bytes(req.room)
                 dirty = True
             if not active:
-                if queue and queue[0].arrival > now:
-                    self.sleep(min(queue[0].arrival - now, 0.05))
-                    continue
-                if queue:    # the next request does not fit even alone
-                    raise RuntimeError(f"request {queue[0].rid} exceeds the memory budget")
+                if queue:
+                    self.sleep(min(max(queue[0].arrival - now, 0.0), 0.05))
                 continue
             if dirty:
                 batch.set([s for _, s, _ in active], [r.room.n_steps for r, _, _ in active])
                 dirty = False
             batch.step(self.chunk, self.use_graph)
             steps, status = batch.sync()
-            if np.any(status != 0):
-                bad = [active[q][0].rid for q in np.nonzero(status)[0]]
-                raise RuntimeError(f"requests {bad}: pressure diverged (FDTD_ERR_UNSTABLE)")
-            finished = [q for q, (r, _, _) in enumerate(active) if steps[q] >= r.room.n_steps]
-            self.log.append({"t": self.clock() - t0, "active": len(active), "finished": len(finished),
+            now = self.clock() - t0
+            leave: Dict[int, Optional[str]] = {}
+            for q, (r, _, _) in enumerate(active):
+                if status[q] != 0:
+                    leave[q] = f"pressure diverged (FDTD_ERR_UNSTABLE) by step {int(steps[q])}"
+                elif steps[q] >= r.room.n_steps:
+                    leave[q] = None
+                elif r.rid in self._cancelled:
+                    leave[q] = "cancelled"
+                elif late(r, now):
+                    leave[q] = "deadline exceeded"
+            self.log.append({"t": now, "active": len(active),
+                             "finished": sum(1 for e in leave.values() if e is None),
+                             "failed": sum(1 for e in leave.values() if e is not None),
                              "queued": len(queue)})
-            if finished:
-                keep = [a for q, a in enumerate(active) if q not in set(finished)]
-                done = [active[q] for q in finished]
+            if leave:
+                keep = [a for q, a in enumerate(active) if q not in leave]
                 batch.set([s for _, s, _ in keep], [r.room.n_steps for r, _, _ in keep])
-                t_done = self.clock() - t0
-                for req, solver, start in done:
-                    results.append(Result(req.rid, be.traces(solver), req.arrival, start, t_done))
+                for q, err in leave.items():
+                    req, solver, start = active[q]
+                    results.append(Result(req.rid, be.traces(solver), req.arrival, start, now, error=err))
                     used -= room_bytes(req.room)
                     be.release(solver)
                 active = keep
@@ -264,9 +320,13 @@ class SequentialServer:
                 self.sleep(req.arrival - now)
             start = self.clock() - t0
             solver = be.make(req.room)
-            be.run_plain(solver, req.room.n_steps)
+            err = None
+            try:
+                be.run_plain(solver, req.room.n_steps)
+            except RuntimeError as e:          # FDTD_ERR_UNSTABLE: this request only
+                err = f"pressure diverged: {e}"
             traces = be.traces(solver)
-            results.append(Result(req.rid, traces, req.arrival, start, self.clock() - t0))
+            results.append(Result(req.rid, traces, req.arrival, start, self.clock() - t0, error=err))
             be.release(solver)
         return sorted(results, key=lambda r: r.rid)
 

@@ -18,9 +18,11 @@ class FakeClock:
 
 
 class FakeSolver:
-    def __init__(self, room):
+    def __init__(self, room, diverge_at=None):
         self.room = room
         self.step = 0
+        self.diverge_at = diverge_at      # a step whose pressure goes non-finite
+        self.unstable = False
 
 
 class FakeBatch:
@@ -44,17 +46,27 @@ class FakeBatch:
 
     def step(self, n, use_graph=True):
         for m, lim in zip(self.members, self.limits):
-            m.step = min(lim, m.step + n)
+            if m.unstable:
+                continue
+            target = min(lim, m.step + n)
+            if m.diverge_at is not None:
+                check = (m.diverge_at // 256 + 1) * 256     # the first 256-step check after it
+                if check <= target:
+                    m.step, m.unstable = check, True
+                    continue
+            m.step = target
         self.clock.t += self.cost * n
 
     def sync(self):
         return (np.array([m.step for m in self.members], np.int32),
-                np.zeros(len(self.members), np.int32))
+                np.array([-3 if m.unstable else 0 for m in self.members], np.int32))
 
 
 class FakeBackend:
-    def __init__(self, clock, budget=1 << 40):
+    def __init__(self, clock, budget=1 << 40, diverge=None, alloc_fail=()):
         self.clock, self.budget = clock, budget
+        self.diverge = diverge or {}          # id(room) -> step that goes non-finite
+        self.alloc_fail = {id(r) for r in alloc_fail}
         self.made = []
         self.peak = 0
         self.live = 0
@@ -65,12 +77,14 @@ class FakeBackend:
         return self.budget
 
     def make(self, room):
+        if id(room) in self.alloc_fail:
+            raise MemoryError("fake: out of device memory")
         self.made.append(room)
         self.live += 1
         self.peak = max(self.peak, self.live)
         self.live_bytes += room_bytes(room)
         self.peak_bytes = max(self.peak_bytes, self.live_bytes)
-        return FakeSolver(room)
+        return FakeSolver(room, self.diverge.get(id(room)))
 
     def batch(self):
         return FakeBatch(self.clock)
@@ -147,3 +161,91 @@ def test_sequential_server_and_summary():
     starts = sorted(r.start for r in res)
     finishes = sorted(r.finish for r in res)
     assert all(b >= a for a, b in zip(finishes[:-1], starts[1:]))   # one at a time
+
+
+def test_unstable_request_leaves_alone():
+    """A room whose pressure diverges stops at its check step and leaves with
+    an error and the traces it recorded; every other room completes."""
+    clock = FakeClock()
+    reqs = mixed_room_requests(10, seed=2, steps=(600, 900), axes=(32, 48))
+    bad = reqs[3]
+    be = FakeBackend(clock, diverge={id(bad.room): 300})
+    res = BatchServer(max_slots=4, chunk=64, backend=be, clock=clock, sleep=clock.sleep).run(reqs)
+    assert [r.rid for r in res] == sorted(r.rid for r in reqs)
+    for r in res:
+        q = next(x for x in reqs if x.rid == r.rid)
+        if q is bad:
+            assert r.error is not None and "UNSTABLE" in r.error and "512" in r.error
+            assert r.traces.shape[0] == 512
+        else:
+            assert r.ok and r.traces.shape[0] == q.room.n_steps
+    assert be.live == 0                                   # every solver released
+    s = summarize(res, work=1.0)
+    assert s["requests"] == 9 and s["failed"] == 1
+
+
+def test_sequential_server_isolates_a_diverging_request():
+    clock = FakeClock()
+    reqs = small_requests(6)
+
+    class Diverging(FakeBackend):
+        def run_plain(self, solver, n):
+            if solver.room is reqs[2].room:
+                raise RuntimeError("AcousticFDTD: pressure diverged (FDTD_ERR_UNSTABLE)")
+            super().run_plain(solver, n)
+
+    res = SequentialServer(backend=Diverging(clock), clock=clock, sleep=clock.sleep).run(reqs)
+    errs = {r.rid: r.error for r in res}
+    assert errs[reqs[2].rid] is not None
+    assert sum(e is None for e in errs.values()) == 5
+
+
+def test_cancel_queued_and_running_requests():
+    clock = FakeClock()
+    reqs = mixed_room_requests(8, seed=4, steps=(2000, 3000), axes=(32,))
+    for i, r in enumerate(reqs):
+        r.arrival = 0.01 * i
+    srv = BatchServer(max_slots=2, chunk=64, backend=FakeBackend(clock), clock=clock, sleep=clock.sleep)
+    running, queued = reqs[0].rid, reqs[7].rid
+    srv.cancel(queued)                       # dropped before it is admitted
+
+    class Batch(FakeBatch):                  # cancels reqs[0] after its first chunk
+        def step(self, n, use_graph=True):
+            super().step(n, use_graph)
+            srv.cancel(running)
+
+    srv.backend.batch = lambda: Batch(clock)
+    res = {r.rid: r for r in srv.run(reqs)}
+    assert res[queued].error == "cancelled" and res[queued].traces.shape[0] == 0
+    assert res[running].error == "cancelled" and 0 < res[running].traces.shape[0] < reqs[0].room.n_steps
+    assert all(res[q.rid].ok for q in reqs[1:7])
+
+
+def test_deadline_evicts_and_rejects():
+    clock = FakeClock()
+    reqs = mixed_room_requests(6, seed=5, steps=(1000, 1000), axes=(32,))
+    for r in reqs:
+        r.arrival = 0.0
+    reqs[0].deadline = 0.03          # runs, but needs 1000 x 1e-4 s = 0.1 s
+    reqs[5].deadline = 0.01          # still queued behind the two slots when it expires
+    srv = BatchServer(max_slots=2, chunk=50, backend=FakeBackend(clock), clock=clock, sleep=clock.sleep)
+    res = {r.rid: r for r in srv.run(reqs)}
+    assert res[reqs[0].rid].error == "deadline exceeded"
+    assert 0 < res[reqs[0].rid].traces.shape[0] < 1000
+    assert res[reqs[5].rid].error == "deadline exceeded" and res[reqs[5].rid].traces.shape[0] == 0
+    assert all(res[q.rid].ok for q in reqs[1:5])
+
+
+def test_allocation_failure_and_oversized_request_are_rejected():
+    clock = FakeClock()
+    reqs = mixed_room_requests(6, seed=6, steps=(100, 200), axes=(32,))
+    big = Request(99, mixed_room_requests(1, seed=7, steps=(100, 100), axes=(128,))[0].room)
+    budget = 3 * max(room_bytes(r.room) for r in reqs)
+    assert room_bytes(big.room) > budget
+    be = FakeBackend(clock, budget=budget, alloc_fail=[reqs[1].room])
+    res = {r.rid: r for r in BatchServer(max_slots=4, chunk=32, backend=be, clock=clock,
+                                        sleep=clock.sleep).run(reqs + [big])}
+    assert res[99].error == "exceeds the memory budget"
+    assert res[reqs[1].rid].error.startswith("allocation failed")
+    assert sum(r.ok for r in res.values()) == 5
+    assert be.peak_bytes <= budget

@@ -96,7 +96,7 @@ def test_batch_latches_instability(cuda):
     b.set(s, [300, 300])
     b.step(300)
     steps, status = b.sync()
-    assert list(steps) == [300, 300]
+    assert list(steps) == [300, 256]          # the diverged member stopped at its check step
     assert status[0] == 0 and status[1] == -3
 
 
@@ -111,3 +111,76 @@ def test_batch_server_matches_sequential(cuda):
     for a, b in zip(seq, bat):
         assert a.rid == b.rid
         assert bits_equal(a.traces, b.traces), a.rid
+
+
+def nan_signal(room, at):
+    sig = np.array(room.signal(), np.float32)
+    sig[at] = np.nan
+    return sig
+
+
+def test_unstable_member_stops_like_a_single_room(cuda):
+    """A NaN planted in one room's source: in the batch that room stops at the
+    first 256-step check after it, in exactly the state the single-room step
+    leaves when it returns UNSTABLE; the other rooms finish as if alone."""
+    from spectral_analyzer_b200.serving import EngineBatch, make_solver
+    rs = [seeded_room(40, 36, 48, 700, seed=11, n_rec=2, n_pml=4),
+          seeded_room(64, 48, 40, 600, seed=12, n_rec=3, n_pml=4, source_kind="ricker"),
+          seeded_room(33, 50, 27, 650, seed=13, n_rec=2, n_pml=4)]
+    bad = 1
+    sig = nan_signal(rs[bad], 30)
+    f = make_solver(rs[bad])
+    f.set_point_source(rs[bad].src_flat, sig)
+    f.set_kernel("fused")
+    assert f.step_rc(rs[bad].n_steps) == -3
+    assert f.step_count == 256
+    ref_bad = (f.get_traces(), f.get_pressure_field(), f.get_velocity_x())
+    ref = [alone(r) if q != bad else None for q, r in enumerate(rs)]
+
+    solvers = [make_solver(r) for r in rs]
+    solvers[bad].set_point_source(rs[bad].src_flat, sig)
+    b = EngineBatch()
+    b.set(solvers, [r.n_steps for r in rs])
+    b.step(300, True)
+    steps, status = b.sync()
+    assert list(status) == [0, -3, 0] and steps[bad] == 256
+    b.step(100, True)                       # the stopped member does not move
+    steps, status = b.sync()
+    assert steps[bad] == 256 and status[bad] == -3
+    t, P, Vx = ref_bad
+    assert bits_equal(solvers[bad].get_traces(), t)
+    assert bits_equal(solvers[bad].get_pressure_field(), P)
+    assert bits_equal(solvers[bad].get_velocity_x(), Vx)
+    keep = [s for q, s in enumerate(solvers) if q != bad]
+    b.set(keep, [r.n_steps for q, r in enumerate(rs) if q != bad])
+    while True:
+        b.step(128, True)
+        steps, status = b.sync()
+        if np.all(steps >= [r.n_steps for q, r in enumerate(rs) if q != bad]):
+            break
+    b.set([], [])
+    for q in (0, 2):
+        tr, P, Vz = ref[q]
+        assert bits_equal(solvers[q].get_traces(), tr)
+        assert bits_equal(solvers[q].get_pressure_field(), P)
+
+
+def test_server_isolates_a_diverging_request(cuda):
+    """BatchServer on the engine: the NaN request leaves with an error, the rest
+    return the traces they have alone."""
+    from spectral_analyzer_b200.serving import BatchServer, Request, _EngineBackend
+    rs = [seeded_room(40, 36, 48, 600, seed=21 + q, n_rec=2, n_pml=4) for q in range(4)]
+    reqs = [Request(q, r) for q, r in enumerate(rs)]
+
+    class Planted(_EngineBackend):
+        def make(self, room):
+            f = super().make(room)
+            if room is rs[2]:
+                f.set_point_source(room.src_flat, nan_signal(room, 10))
+            return f
+
+    res = BatchServer(max_slots=4, chunk=64, backend=Planted()).run(reqs)
+    assert "UNSTABLE" in res[2].error and res[2].traces.shape[0] == 256
+    for q in (0, 1, 3):
+        assert res[q].ok
+        assert bits_equal(res[q].traces, alone(rs[q])[0])

@@ -120,3 +120,46 @@ def test_instability_is_reported_on_every_slab():
     with pytest.raises(RuntimeError, match="FDTD_ERR_UNSTABLE"):
         run.step(300)
     assert run.step_count == 256
+
+
+def _leaving_rank_main(rank, world, port, out_path, leave_at):
+    """Rank 1 leaves between steps (after ``leave_at`` steps, nothing in flight);
+    rank 0 learns of it from its next halo exchange, which ends with an error
+    within the process group's short timeout instead of waiting for good."""
+    import time
+    import torch.distributed as dist
+    from datetime import timedelta
+    from slab_numpy import NumpySlab
+    from spectral_analyzer_b200.slab import DistExchange
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=5))
+    room = edge_room(13, 60)
+    ranges = partition(room.nx, world)
+    a, b = ranges[rank]
+    slab = NumpySlab(room, a, b, [])
+    run = SlabRunner([slab], DistExchange(slab, rank, world))
+    if rank == 1:
+        run.step(leave_at)
+        dist.destroy_process_group()
+        return
+    t0 = time.monotonic()
+    err = ""
+    try:
+        run.step(room.n_steps)
+    except Exception as e:           # the collective's error (peer gone or timeout)
+        err = f"{type(e).__name__}: {e}"
+    with open(out_path, "w") as fh:
+        fh.write(f"{run.step_count}\n{time.monotonic() - t0:.3f}\n{err}\n")
+
+
+def test_rank_that_leaves_is_detected_by_the_others():
+    import torch.multiprocessing as mp
+    with tempfile.TemporaryDirectory() as d:
+        out = os.path.join(d, "r0.txt")
+        mp.start_processes(_leaving_rank_main, args=(2, _free_port(), out, 7), nprocs=2, join=True,
+                           start_method="spawn")
+        steps, secs, err = open(out).read().split("\n", 2)
+    assert err.strip(), "rank 0 finished although its neighbour left"
+    assert int(steps) == 7                       # it stopped at the step its neighbour did not take
+    assert float(secs) < 30.0
