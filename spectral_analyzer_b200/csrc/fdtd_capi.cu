@@ -164,6 +164,9 @@ struct AcousticFDTDState {
     long long* h_sidx = nullptr;
     float* h_sw = nullptr;
     float* h_sout = nullptr;
+    // what d_sidx / d_sw hold (upload_taps skips a copy of the same taps)
+    std::vector<long long> up_idx;
+    std::vector<float> up_w;
 
     long long pad(int i, int j, int k) const { return ((long long)i * Ny + j) * g.sz + k; }
     float* P() const { return p[cur]; }
@@ -309,6 +312,8 @@ int ensure_scratch(AcousticFDTDState* st, size_t n)
     st->d_sidx = nullptr; st->d_sw = st->d_sout = nullptr;
     st->h_sidx = nullptr; st->h_sw = st->h_sout = nullptr;
     st->s_cap = 0;
+    st->up_idx.clear();
+    st->up_w.clear();
     CK(cudaMalloc(&st->d_sidx, cap * sizeof(long long)));
     CK(cudaMalloc(&st->d_sw, cap * sizeof(float)));
     CK(cudaMalloc(&st->d_sout, cap * sizeof(float)));
@@ -319,6 +324,23 @@ int ensure_scratch(AcousticFDTDState* st, size_t n)
     return FDTD_OK;
 }
 
+// Copies the n taps staged in h_sidx / h_sw to the device unless it already
+// holds exactly these (a caller sampling the same receivers every step).
+int upload_taps(AcousticFDTDState* st, size_t n, cudaStream_t s)
+{
+    if (n == 0) return FDTD_OK;
+    if (st->up_idx.size() == n && memcmp(st->up_idx.data(), st->h_sidx, n * sizeof(long long)) == 0 &&
+        memcmp(st->up_w.data(), st->h_sw, n * sizeof(float)) == 0)
+        return FDTD_OK;
+    st->up_idx.clear();
+    st->up_w.clear();
+    CK(cudaMemcpyAsync(st->d_sidx, st->h_sidx, n * sizeof(long long), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(st->d_sw, st->h_sw, n * sizeof(float), cudaMemcpyHostToDevice, s));
+    st->up_idx.assign(st->h_sidx, st->h_sidx + n);
+    st->up_w.assign(st->h_sw, st->h_sw + n);
+    return FDTD_OK;
+}
+
 // Weighted gathers already staged in h_sidx / h_sw (n_out * taps entries):
 // runs k_wsum on `field` and copies n_out results to `out`.
 int run_wsum(AcousticFDTDState* st, const float* field, int n_out, int taps, int from_zero,
@@ -326,10 +348,7 @@ int run_wsum(AcousticFDTDState* st, const float* field, int n_out, int taps, int
 {
     if (n_out <= 0) return FDTD_OK;
     const size_t n = (size_t)n_out * taps;
-    if (n > 0) {
-        CK(cudaMemcpyAsync(st->d_sidx, st->h_sidx, n * sizeof(long long), cudaMemcpyHostToDevice, st->stream));
-        CK(cudaMemcpyAsync(st->d_sw, st->h_sw, n * sizeof(float), cudaMemcpyHostToDevice, st->stream));
-    }
+    if (int rc = upload_taps(st, n, st->stream)) return rc;
     CK(launch_wsum(field, st->d_sidx, st->d_sw, n_out, taps, from_zero, st->d_sout, st->stream));
     ++st->launches;
     CK(cudaMemcpyAsync(st->h_sout, st->d_sout, (size_t)n_out * sizeof(float), cudaMemcpyDeviceToHost,
@@ -1894,8 +1913,7 @@ int substep_plate(AcousticFDTDState* st, int n_saddle, float* out)
     // saddle samples (taps staged by the caller) from the new displacement
     if (n_saddle > 0) {
         const size_t n = (size_t)n_saddle * 4;
-        CK(cudaMemcpyAsync(st->d_sidx, st->h_sidx, n * sizeof(long long), cudaMemcpyHostToDevice, s));
-        CK(cudaMemcpyAsync(st->d_sw, st->h_sw, n * sizeof(float), cudaMemcpyHostToDevice, s));
+        if (int rc2 = upload_taps(st, n, s)) return rc2;
         CK(launch_wsum(st->d_w[st->wi_cur], st->d_sidx, st->d_sw, n_saddle, 4, 0, st->d_sout, s));
         ++st->launches;
         CK(cudaMemcpyAsync(st->h_sout, st->d_sout, (size_t)n_saddle * sizeof(float), cudaMemcpyDeviceToHost, s));
