@@ -134,3 +134,25 @@ def test_compiled_reference_matches_fixture(golden):
     idx, w = f.precompute_pressure_samplers(room.receiver_xyz())
     trace = f.run(room.n_steps, room.src_flat, room.signal(), idx, w)
     assert bits_equal(trace, arrays["odd37/trace"])
+
+
+def test_large_room_fixture_describes_the_bench_room():
+    """The 500-step reference prefix of the 512x384x256 room (checked against the
+    engine on the GPU) belongs to the room the benchmark builds."""
+    import json
+    import os
+    from spectral_analyzer_b200.rooms import large_room
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    with open(os.path.join(here, "large_room_prefix.json")) as fh:
+        meta = json.load(fh)
+    with np.load(os.path.join(here, "large_room_prefix.npz")) as z:
+        trace, idx8, wgt8 = z["trace"], z["idx8"], z["wgt8"]
+    room = large_room(n_steps=500)
+    assert json.loads(json.dumps(room.describe())) == meta["room"]
+    assert trace.shape == (500, 8) and trace.dtype == np.float32
+    assert idx8.size == 64 and wgt8.size == 64
+    assert np.abs(trace).max() > 0 and meta["steps"] == 500
+    # the oracle's samplers are the reference's
+    o = OracleFDTD(room.nx, room.ny, room.nz, room.dx, n_pml=room.n_pml)
+    idx, w = o.precompute_pressure_samplers(room.receiver_xyz())
+    assert np.array_equal(idx, idx8) and bits_equal(w, wgt8)

@@ -212,6 +212,33 @@ def test_large_room_fused_equals_two_pass(torch_cuda):
     assert torch.equal(out["fused"][1].view(torch.int32), out["two_pass"][1].view(torch.int32))
 
 
+@pytest.mark.parametrize("kernel", ["fused", "two_pass"])
+def test_large_room_500_steps_match_reference(torch_cuda, kernel):
+    """The 512x384x256 bench room for 500 steps: receiver traces and final fields
+    bit for bit against the compiled reference's own run
+    (tests/golden/make_large_golden.py)."""
+    import json
+    import os
+    here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    with open(os.path.join(here, "large_room_prefix.json")) as fh:
+        meta = json.load(fh)
+    with np.load(os.path.join(here, "large_room_prefix.npz")) as z:
+        ref, idx8, wgt8 = z["trace"], z["idx8"], z["wgt8"]
+    room = large_room(n_steps=500)
+    f = engine_room(room, kernel)
+    idx, w = f.precompute_pressure_samplers(room.receiver_xyz())
+    assert np.array_equal(idx, idx8) and bits_equal(w, wgt8)
+    tr = f.run(room.n_steps, room.src_flat, room.signal(), idx, w)
+    assert rel_l2(tr, ref) <= TRACE_TOL
+    assert bits_equal(tr, ref), first_mismatch(tr, ref)
+    h = meta["sha256"]
+    assert sha(f.get_pressure_field()) == h["P"]
+    assert sha(f.get_velocity_x()) == h["Vx"]
+    assert sha(f.get_velocity_y()) == h["Vy"]
+    assert sha(f.get_velocity_z()) == h["Vz"]
+    f.close()
+
+
 def test_large_room_superposition(torch_cuda):
     """Size-independent property at full size: the step is linear in the source
     signal.  Doubling the signal doubles every trace and the traces of two
