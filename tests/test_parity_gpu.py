@@ -213,18 +213,20 @@ def test_large_room_fused_equals_two_pass(torch_cuda):
 
 
 @pytest.mark.parametrize("kernel", ["fused", "two_pass"])
-def test_large_room_500_steps_match_reference(torch_cuda, kernel):
-    """The 512x384x256 bench room for 500 steps: receiver traces and final fields
-    bit for bit against the compiled reference's own run
-    (tests/golden/make_large_golden.py)."""
+@pytest.mark.parametrize("name,steps", [("large_room_prefix", 500), ("large_room_10000", 10000)])
+def test_large_room_matches_reference(torch_cuda, kernel, name, steps):
+    """The 512x384x256 bench room for 500 and for all 10000 steps: receiver
+    traces and final fields bit for bit against the compiled reference's own
+    run (tests/golden/make_large_golden.py)."""
     import json
     import os
     here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-    with open(os.path.join(here, "large_room_prefix.json")) as fh:
+    with open(os.path.join(here, name + ".json")) as fh:
         meta = json.load(fh)
-    with np.load(os.path.join(here, "large_room_prefix.npz")) as z:
+    with np.load(os.path.join(here, name + ".npz")) as z:
         ref, idx8, wgt8 = z["trace"], z["idx8"], z["wgt8"]
-    room = large_room(n_steps=500)
+    room = large_room(n_steps=steps)
+    assert meta["steps"] == steps
     f = engine_room(room, kernel)
     idx, w = f.precompute_pressure_samplers(room.receiver_xyz())
     assert np.array_equal(idx, idx8) and bits_equal(w, wgt8)
