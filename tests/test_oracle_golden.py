@@ -136,22 +136,26 @@ def test_compiled_reference_matches_fixture(golden):
     assert bits_equal(trace, arrays["odd37/trace"])
 
 
-def test_large_room_fixture_describes_the_bench_room():
-    """The 500-step reference prefix of the 512x384x256 room (checked against the
-    engine on the GPU) belongs to the room the benchmark builds."""
+@pytest.mark.parametrize("name,steps", [("large_room_prefix", 500), ("large_room_10000", 10000)])
+def test_large_room_fixture_describes_the_bench_room(name, steps):
+    """The reference runs of the 512x384x256 room (checked against the engine on
+    the GPU) belong to the room the benchmark builds; the 500-step one is the
+    prefix of the 10000-step one."""
     import json
     import os
     from spectral_analyzer_b200.rooms import large_room
     here = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-    with open(os.path.join(here, "large_room_prefix.json")) as fh:
+    with open(os.path.join(here, name + ".json")) as fh:
         meta = json.load(fh)
-    with np.load(os.path.join(here, "large_room_prefix.npz")) as z:
+    with np.load(os.path.join(here, name + ".npz")) as z:
         trace, idx8, wgt8 = z["trace"], z["idx8"], z["wgt8"]
-    room = large_room(n_steps=500)
+    room = large_room(n_steps=steps)
     assert json.loads(json.dumps(room.describe())) == meta["room"]
-    assert trace.shape == (500, 8) and trace.dtype == np.float32
+    assert trace.shape == (steps, 8) and trace.dtype == np.float32
     assert idx8.size == 64 and wgt8.size == 64
-    assert np.abs(trace).max() > 0 and meta["steps"] == 500
+    assert np.abs(trace).max() > 0 and meta["steps"] == steps
+    with np.load(os.path.join(here, "large_room_prefix.npz")) as z:
+        assert bits_equal(trace[:500], z["trace"])
     # the oracle's samplers are the reference's
     o = OracleFDTD(room.nx, room.ny, room.nz, room.dx, n_pml=room.n_pml)
     idx, w = o.precompute_pressure_samplers(room.receiver_xyz())

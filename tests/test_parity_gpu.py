@@ -213,7 +213,7 @@ def test_large_room_fused_equals_two_pass(torch_cuda):
 
 
 @pytest.mark.parametrize("kernel", ["fused", "two_pass"])
-@pytest.mark.parametrize("name,steps", [("large_room_prefix", 500)])
+@pytest.mark.parametrize("name,steps", [("large_room_prefix", 500), ("large_room_10000", 10000)])
 def test_large_room_matches_reference(torch_cuda, kernel, name, steps):
     """The 512x384x256 bench room for 500 and for all 10000 steps: receiver
     traces and final fields bit for bit against the compiled reference's own
