@@ -17,7 +17,7 @@ from __future__ import annotations
 
 import ctypes as C
 import os
-from typing import Optional, Sequence
+from typing import Sequence
 
 import numpy as np
 

@@ -16,7 +16,7 @@ from __future__ import annotations
 import json
 import os
 import time
-from typing import Dict, Optional, Sequence
+from typing import Dict, Sequence
 
 CANDIDATES = (0, 16, 32, 64, 128)
 TILES = (128, 64)

@@ -25,15 +25,14 @@ kernel) ends the run.
 from __future__ import annotations
 
 import ctypes as C
-import math
 import time
 from collections import deque
-from dataclasses import dataclass, field
+from dataclasses import dataclass
 from typing import Callable, Dict, List, Optional, Sequence
 
 import numpy as np
 
-from .rooms import Room, reference_dt
+from .rooms import Room
 
 GRID_AXES = tuple(range(32, 257, 16))
 

@@ -1,7 +1,6 @@
 """Scheduler logic of the serving loop, on the CPU with a fake engine backend."""
 import numpy as np
 
-from spectral_analyzer_b200.rooms import Room
 from spectral_analyzer_b200.serving import (BatchServer, Request, SequentialServer, mixed_room_requests,
                                             poisson_arrivals, room_bytes, summarize)
 

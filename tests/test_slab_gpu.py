@@ -1,7 +1,6 @@
 """CUDA slab kernels: a room split into slabs (stepped in one process with
 plane-copy exchanges), with the fused single-pass kernel or the two passes,
 equals the whole-room engine bit for bit."""
-import numpy as np
 import pytest
 
 from conftest import bits_equal, first_mismatch
