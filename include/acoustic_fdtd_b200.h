@@ -248,18 +248,25 @@ FDTD_B200_API int fdtd_b200_profile_read(AcousticFDTDState* st, double* total_ms
                                          long long* launches, long long* kernel_launches);
 
 /* No counterpart in the reference.  fdtd_sample_pressure_precomputed for
- * callers that cannot allocate — a real-time audio callback sampling the
- * microphones (an allocation may block on driver locks) or code recording a
- * CUDA stream capture.  It never calls cudaMalloc/cudaFree or any allocating
- * routine: its index/weight inputs and its results are staged in one fixed
- * device array (272 KB, shared by all handles on a device and kept until the
- * process exits).  At most 4096 receivers per call (FDTD_ERR_ARG beyond, with
- * the reason in fdtd_b200_last_error).  The first call on a device looks up
- * the array's device address; make that first call before any stream
- * capture.  Each call overwrites what it uses of the array, so nothing in it
- * has to start at zero, but calls that overlap on the GPU (other threads or
- * streams) race on it.  Same arguments, indices checks and results as
- * fdtd_sample_pressure_precomputed; returns after the values are in out_p. */
+ * callers that cannot allocate — e.g. a real-time audio callback sampling the
+ * microphones, where a cudaMalloc or cudaMallocHost may block on driver locks
+ * for an unbounded time.  It never calls cudaMalloc/cudaFree or any
+ * allocating routine: its index/weight inputs and its results are staged in
+ * one fixed device array (272 KB, shared by all handles on a device and kept
+ * until the process exits).  At most 4096 receivers per call (FDTD_ERR_ARG
+ * beyond, with the reason in fdtd_b200_last_error).  The first call on a
+ * device looks up the array's device address (cudaGetSymbolAddress) and
+ * keeps it for the life of the process; make that first call before any CUDA
+ * stream capture starts, and do not use this function after a
+ * cudaDeviceReset of that device in the same process (the kept address is
+ * then stale).  The call copies from and to pageable host memory on the
+ * handle's stream and ends with a synchronisation of that stream: it blocks
+ * until every step already queued on the handle has finished, so a real-time
+ * caller should call it only when no steps are queued, and it must not be
+ * made while the handle's stream is being captured.  Each call overwrites
+ * what it uses of the array, so nothing in it has to start at zero, but calls
+ * that overlap on the GPU (other threads or streams) race on it.  Same
+ * arguments, index checks and results as fdtd_sample_pressure_precomputed. */
 FDTD_B200_API int fdtd_b200_sample_pressure_noalloc(const AcousticFDTDState* st, int n_rec,
                                                    const int* idx8, const float* wgt8,
                                                    float* out_p);

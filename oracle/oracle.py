@@ -122,7 +122,7 @@ def _load_ref(fast: bool = False):
     if key not in _lib_cache:
         path = REF_LIB_V3 if (fast and os.path.exists(REF_LIB_V3) and _host_has_avx2_fma()) else REF_LIB
         if not os.path.exists(path):
-            raise RuntimeError(f"compiled reference missing: {path} (build it with `make -C oracle`)")
+            raise RuntimeError(f"compiled reference missing: {path} (build it with `make -C oracle REF=<reference checkout>`)")
         lib = C.CDLL(path)
         # the reference's own names: fdtd_<name>
         _bind_common(lib, "fdtd_", C.c_float, _f32p)

@@ -1,5 +1,7 @@
 """Plain PyTorch restatement of the per-cell-absorption room, differentiated by
 torch.autograd: the reference the adjoint kernels are checked against.
+Test infrastructure only (imported by tests/ as a checker, never by the
+engine).
 
 Same model as fdtd_adjoint.cu (the reference's update,
 csrc/kernels/acoustic_fdtd.cpp:1099-1148 and :894-952/:1176-1234, with

@@ -1451,10 +1451,13 @@ const char* fdtd_b200_last_error(void) { return g_err; }
 /*
  * Some callers cannot allocate: the instrument co-evolver samples its
  * microphones once per audio sample from a real-time audio callback, where a
- * cudaMalloc/cudaMallocHost may block on driver locks for an unbounded time,
- * and a caller that is recording a CUDA stream capture may not allocate at
- * all.  fdtd_sample_pressure_precomputed grows per-handle scratch on demand;
- * this variant stages its inputs and result in one fixed device array instead.
+ * cudaMalloc/cudaMallocHost may block on driver locks for an unbounded time.
+ * fdtd_sample_pressure_precomputed grows per-handle scratch on demand; this
+ * variant stages its inputs and result in one fixed device array instead.
+ * It ends with a synchronisation of the handle's stream (so it also waits for
+ * steps queued there, and cannot be called while that stream is captured).
+ * The array's device address is looked up on the first call on a device and
+ * kept; a cudaDeviceReset of that device makes the kept address stale.
  */
 namespace {
 
@@ -1507,7 +1510,13 @@ extern "C" int fdtd_b200_sample_pressure_noalloc(const AcousticFDTDState* cst, i
         return FDTD_ERR_ARG;
     }
     for (long long q = 0; q < (long long)n_rec * 8; ++q)
-        if (idx8[q] < 0 || idx8[q] >= st->N) return FDTD_ERR_ARG;
+        if (idx8[q] < 0 || idx8[q] >= st->N) {
+            std::lock_guard<std::mutex> lk(g_err_mu);
+            snprintf(g_err, sizeof(g_err),
+                     "fdtd_b200_sample_pressure_noalloc: tap %lld (receiver %lld) has index %d outside [0, %lld)",
+                     q, q / 8, idx8[q], (long long)st->N);
+            return FDTD_ERR_ARG;
+        }
     if (dev_guard(st)) return FDTD_ERR_CUDA;
     if (st->device < 0 || st->device >= 64) return FDTD_ERR_ARG;
     NoAllocScratch* s;

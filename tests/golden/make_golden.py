@@ -6,7 +6,7 @@ compiled unchanged by oracle/Makefile (oracle/_ref/libfdtd_ref.so, plus the
 deposit and per-face absorption hooks of oracle/ref_shim.cpp), run here on
 seeded inputs.  Run from the repository root:
 
-    make -C oracle && python tests/golden/make_golden.py
+    make -C oracle REF=<reference checkout> && python tests/golden/make_golden.py
 
 Writes tests/golden/reference_fixtures.npz (arrays) and
 tests/golden/reference_fixtures.json (SHA-256 of large final fields, return

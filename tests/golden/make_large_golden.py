@@ -7,7 +7,7 @@ per-face absorption hooks of oracle/ref_shim.cpp), here on the host cores
 (about four minutes on 8 threads; the full 10000-step run about 80).  Run
 from the repository root:
 
-    make -C oracle && python tests/golden/make_large_golden.py [steps]
+    make -C oracle REF=<reference checkout> && python tests/golden/make_large_golden.py [steps]
 
 Writes tests/golden/large_room_prefix.npz (the steps x 8 receiver traces and
 the sampler taps) and tests/golden/large_room_prefix.json (SHA-256 of the

@@ -34,7 +34,7 @@ def test_torch_reference_matches_double_oracle():
     torch = pytest.importorskip("torch")
     from oracle import OracleFDTD
     from spectral_analyzer_b200.precision import pressure_taps
-    from spectral_analyzer_b200.torch_reference import traces
+    from torch_reference import traces
     p = small_problem()
     nx, ny, nz = p.shape
     idx, w = pressure_taps(nx, ny, nz, np.asarray(p.receivers, np.float32))
@@ -49,7 +49,7 @@ def test_torch_reference_matches_double_oracle():
 def test_torch_reference_gradient_matches_finite_differences():
     torch = pytest.importorskip("torch")
     from spectral_analyzer_b200.precision import pressure_taps
-    from spectral_analyzer_b200.torch_reference import loss_and_grad, traces
+    from torch_reference import loss_and_grad, traces
     p = small_problem(n=(12, 11, 14), steps=60, n_pml=3)
     nx, ny, nz = p.shape
     idx, w = pressure_taps(nx, ny, nz, np.asarray(p.receivers, np.float32))

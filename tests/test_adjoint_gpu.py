@@ -49,7 +49,7 @@ def test_float_forward_is_the_oracle(cuda):
 
 def test_double_adjoint_is_torch_autograd(cuda):
     from spectral_analyzer_b200.adjoint import AdjointRoom
-    from spectral_analyzer_b200.torch_reference import loss_and_grad
+    from torch_reference import loss_and_grad
     prob = problem(n=(28, 24, 30), steps=220, n_pml=5)
     tgt = targets_for(prob)
     r = AdjointRoom(prob, double=True, checkpoint_every=50)
