@@ -264,7 +264,9 @@ __device__ __forceinline__ void acquire_tensormap(const CUtensorMap* map)
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(map) : "memory");
 }
 
-template <class C>
+// PEER = false compiles out the neighbour ghost-plane stores (single rooms and
+// batches), which the slab step of a split room needs.
+template <class C, bool PEER = true>
 __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap* tmP,
                                            const CUtensorMap* tmX, const CUtensorMap* tmY,
                                            const CUtensorMap* tmZ, int tile, int seg, int seg_len,
@@ -421,6 +423,10 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
         }
         pph ^= 1u << ps;
         vph ^= 1u << vsg;
+        // iteration u+D's loads go into the slots iteration u-1 freed (their last
+        // reads came before the barrier above), so thread 0 issues them before
+        // its own work of this iteration rather than after it
+        if (tid == 0 && u + C::D <= u1) issue(u + C::D, pslot[C::RING - 1], vslot[C::VSTAGES - 1]);
         const float ax_next = ax_at(u + 1), px_next = px_at(u - 2);
         const float* vs = smem + C::VST0 + vsg * C::V_STAGE;
 
@@ -453,7 +459,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                     stg4(a.vout[0] + f * PL + own, vnew);
 #pragma unroll
                     for (int sd = 0; sd < 2; ++sd)   // the neighbours' ghost faces
-                        if (a.pr.vx[sd] && f >= a.pr.v_lo[sd] && f < a.pr.v_hi[sd])
+                        if (PEER && a.pr.vx[sd] && f >= a.pr.v_lo[sd] && f < a.pr.v_hi[sd])
                             stg4(a.pr.vx[sd] + (f + a.pr.dl[sd]) * PL + own, vnew);
                 }
             }
@@ -582,7 +588,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                         stg4(a.pn + ib + own, out);
 #pragma unroll
                         for (int sd = 0; sd < 2; ++sd)   // the neighbours' ghost planes
-                            if (a.pr.pn[sd] && i >= a.pr.p_lo[sd] && i < a.pr.p_hi[sd])
+                            if (PEER && a.pr.pn[sd] && i >= a.pr.p_lo[sd] && i < a.pr.p_hi[sd])
                                 stg4(a.pr.pn[sd] + (i + a.pr.dl[sd]) * PL + own, out);
                     }
                 }
@@ -604,7 +610,6 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
 #pragma unroll
             for (int q = 0; q + 1 < C::VSTAGES; ++q) vslot[q] = vslot[q + 1];
             vslot[C::VSTAGES - 1] = vfree;
-            if (tid == 0 && u + C::D <= u1) issue(u + C::D, pslot[3 + C::D - 1], vslot[C::D - 1]);
         }
     }
 
@@ -627,7 +632,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
 }
 
 // Single-room step: one CTA per (tile, segment).
-template <class C>
+template <class C, bool PEER>
 __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
                                                       const __grid_constant__ CUtensorMap tmP,
                                                       const __grid_constant__ CUtensorMap tmX,
@@ -647,8 +652,8 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
     init_barriers<C>(bar0);
     Pipe<C> pp;
     pp.init();
-    fused_tile<C>(a, &tmP, &tmX, &tmY, &tmZ, blockIdx.x, blockIdx.y, seg_len, tiles_k, smem, sbase,
-                  bar0, pp);
+    fused_tile<C, PEER>(a, &tmP, &tmX, &tmY, &tmZ, blockIdx.x, blockIdx.y, seg_len, tiles_k, smem, sbase,
+                        bar0, pp);
 }
 
 
@@ -696,7 +701,7 @@ __global__ void __launch_bounds__(C::NT, 2) k_fused_batch(BatchMember* __restric
         a.xs = XSpan{0, 0, 0, 0};
         a.pr = XPeers{};
         const int local = item - m->items_begin;
-        if (!fused_tile<C>(a, &m->maps[par][0], &m->maps[par][1], &m->maps[par][2], &m->maps[par][3],
+        if (!fused_tile<C, false>(a, &m->maps[par][0], &m->maps[par][1], &m->maps[par][2], &m->maps[par][3],
                            local % m->tiles, local / m->tiles, m->seg_len, m->tiles_k, smem, sbase,
                            bar0, pp, true))
             break;
@@ -838,13 +843,16 @@ static cudaError_t launch_step_of(const FusedArgs& a, FusedCache* cache, cudaStr
     if (e != cudaSuccess) return e;
     if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
     if (!g_configured[shape][dev]) {
-        e = cudaFuncSetAttribute(k_fused_step<C>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        e = cudaFuncSetAttribute(k_fused_step<C, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)C::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k_fused_step<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)C::SMEM_BYTES);
         if (e != cudaSuccess) return e;
         e = cudaDeviceGetAttribute(&g_sms[shape][dev], cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
         int slots = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&slots, k_fused_step<C>, C::NT, C::SMEM_BYTES);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&slots, k_fused_step<C, true>, C::NT, C::SMEM_BYTES);
         if (e != cudaSuccess) return e;
         g_slots_per_sm[shape][dev] = slots > 0 ? slots : 1;
         g_configured[shape][dev] = true;
@@ -869,8 +877,13 @@ static cudaError_t launch_step_of(const FusedArgs& a, FusedCache* cache, cudaStr
     const int seg_len = (int)((n_own + segs - 1) / segs);
     segs = (n_own + seg_len - 1) / seg_len;
     dim3 grid((unsigned)tiles, (unsigned)segs, 1);
-    k_fused_step<C><<<grid, C::NT, C::SMEM_BYTES, s>>>(a, maps[0], maps[1], maps[2], maps[3], seg_len,
-                                                       tiles_k);
+    const bool peer = a.pr.pn[0] || a.pr.pn[1] || a.pr.vx[0] || a.pr.vx[1];
+    if (peer)
+        k_fused_step<C, true><<<grid, C::NT, C::SMEM_BYTES, s>>>(a, maps[0], maps[1], maps[2], maps[3], seg_len,
+                                                                 tiles_k);
+    else
+        k_fused_step<C, false><<<grid, C::NT, C::SMEM_BYTES, s>>>(a, maps[0], maps[1], maps[2], maps[3], seg_len,
+                                                                  tiles_k);
     return cudaGetLastError();
 }
 
