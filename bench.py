@@ -20,9 +20,13 @@ Lines printed (rank 0, one JSON object):
             pool over all host cores) on a time-bounded sample of the same room.
 
 --impl reference times the reference's CPU solver alone (rank 0; other ranks
-exit 0).  Multi-GPU (torchrun): every rank advances its own copy of the room
-(independent replicas, weak scaling); value sums the ranks' cells over the
-slowest rank's time.
+exit 0).  Multi-GPU: `python bench.py --gpus N` launches its N ranks itself
+(torch.distributed.run, one GPU each), or runs under an external torchrun;
+with N > 1 ranks the room is split along i into N slabs (strong scaling: one
+ghost exchange of 3 P planes and 2 Vx faces per side and step over NCCL,
+overlapped with the interior planes); value = the room's cells x steps over
+the slowest rank's device time.  --scale-mode replicas runs N independent
+copies of the room instead (weak scaling).
 """
 from __future__ import annotations
 
@@ -73,6 +77,12 @@ def parse_args():
     ap.add_argument("--decompose", action="store_true",
                     help="split the room into slabs along i (torchrun ranks, or --slabs on one GPU)")
     ap.add_argument("--slabs", type=int, default=2)
+    ap.add_argument("--scale-mode", choices=["split", "replicas"], default="split",
+                    help="N>1: split the room into N slabs along i (strong scaling, one ghost exchange "
+                         "per step overlapped with the interior) or run N independent replicas (weak)")
+    ap.add_argument("--plumbing-check", action="store_true",
+                    help="no GPU: ranks on gloo with a host stand-in for the step, to check the "
+                         "rank launch, the max-over-ranks timing and the JSON line")
     ap.add_argument("--peer", action="store_true",
                     help="with --decompose: the step writes the neighbours' ghost planes itself")
     ap.add_argument("--serve-requests", type=int, default=256)
@@ -599,8 +609,145 @@ def slab_arm(args):
     return 0
 
 
+def launch_ranks(n: int, argv) -> int:
+    """Re-run this script as n ranks (torch.distributed.run, one GPU each) when
+    it was started without a launcher; returns the launcher's exit code."""
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={n}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), os.path.abspath(__file__), *argv]
+    try:
+        return subprocess.call(cmd, timeout=3600)
+    except subprocess.TimeoutExpired:
+        return 124
+
+
+def split_line(args, world, ms_max, e2e, launches, clocks, own_cells, cells, kind):
+    """The JSON line of an N-rank split-room run (rank 0 prints it)."""
+    step_ms = ms_max / args.steps
+    achieved = BYTES_PER_CELL_UPDATE * own_cells / (step_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    return {"metric": METRIC, "value": cells * args.steps / (ms_max / 1e3) / 1e9, "unit": METRIC,
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": kind,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": f"{peak_kind} hbm_gbs",
+                         "kernel": "one rank's whole step (both parts of the fused slab step, the ghost "
+                                   "exchange overlapped with the interior, receivers)",
+                         "algorithmic_bytes_per_step_per_rank": BYTES_PER_CELL_UPDATE * own_cells},
+            "cpu_baseline": None, "e2e": e2e, "gpu_launches": launches, "clocks": clocks}
+
+
+def split_arm(args):
+    """N>1 ranks (torchrun, NCCL): the 512x384x256 room split along i into N
+    slabs (strong scaling).  Each step: the planes the neighbours keep as ghosts,
+    then the interior while 3 P planes and 2 Vx faces per side travel to the
+    neighbours over NCCL on a side stream, then the receivers.  value = the
+    room's cells x steps over the slowest rank's device time; e2e = the same with
+    the source sample given by the host every step (a launch argument) and each
+    rank's receiver samples read back every step."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    world = int(os.environ["WORLD_SIZE"])
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    from spectral_analyzer_b200.slab import distributed_room
+    room = workload()
+    K, W = args.steps, args.warmup
+    room.n_steps = W + 2 * K + 1
+    run = distributed_room(room, rank, world, overlap=True)
+    slab = run.slabs[0]
+    run.step(W)
+    dist.barrier()
+    torch.cuda.synchronize()
+    l0 = slab.launch_count
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(gpu_uuid(local)) as clk:
+        e0.record()
+        run.step(K)
+        e1.record()
+        torch.cuda.synchronize()
+    launches = slab.launch_count - l0
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    # end to end: host source sample in, this rank's receiver samples out, every step
+    sig = room.signal()
+    out = np.zeros(len(slab.rec_ids), np.float32)
+    dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(K):
+        run.step(1, host_sample=lambda q: float(sig[q % len(sig)]))
+        if out.size:
+            slab.read_last(out)
+    torch.cuda.synchronize()
+    t2 = torch.tensor([time.perf_counter() - t0], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t2, op=dist.ReduceOp.MAX)
+    el = float(t2.item())
+    n_rec_all = torch.tensor([out.size], dtype=torch.int64, device="cuda")
+    dist.all_reduce(n_rec_all)
+    e2e = {"value": room.cells * K / el / 1e9, "unit": METRIC, "h2d_bytes_per_step": 4 * world,
+           "d2h_bytes_per_step": 4 * int(n_rec_all.item()), "ms_per_step": el / K * 1e3,
+           "path": "per rank: fdtd_b200_slab_add_pressure (host sample) + slab step + exchange + "
+                   "record + fdtd_b200_slab_read_last"}
+    finite = bool(np.isfinite(run.traces(len(room.receivers))).all())
+    if rank == 0:
+        kind = dict(config_dict(room, world, "fused"), parallelism=f"slab{world}",
+                    exchange="NCCL send/recv of 3 P planes + 2 Vx faces per side, side stream, "
+                             "overlapped with the interior planes")
+        line = split_line(args, world, ms_max, e2e, launches, clk.summary(), slab.own * room.ny * room.nz,
+                          room.cells, kind)
+        line["traces_finite"] = finite
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+    return 0
+
+
+def plumbing_check(args):
+    """No GPU: the launch, the gloo rendezvous, the max-over-ranks timing and the
+    JSON line of a split run, with a host stand-in for the step (checks the
+    bench's multi-rank plumbing on a CPU box; prints no measurement)."""
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist.init_process_group("gloo", timeout=timedelta(seconds=60))
+    from spectral_analyzer_b200.slab import partition
+    room = workload()
+    a, b = partition(room.nx, world)[rank]
+    t0 = time.perf_counter()
+    x = np.zeros(((b - a), 8, 8), np.float32)
+    for _ in range(args.steps):
+        x += 1.0
+        dist.barrier()
+    t = torch.tensor([1e3 * (time.perf_counter() - t0)], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    if rank == 0:
+        kind = dict(config_dict(room, world, "plumbing-check"), parallelism=f"slab{world}")
+        line = split_line(args, world, float(t.item()), None, 0, None, (b - a) * room.ny * room.nz,
+                          room.cells, kind)
+        line["plumbing_check"] = True
+        print(json.dumps(line), flush=True)
+    dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if args.impl == "engine" and args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return launch_ranks(args.gpus, sys.argv[1:])
+    if args.plumbing_check:
+        return plumbing_check(args)
     if args.impl == "reference":
         return reference_arm(args)
     if args.serve:
@@ -611,6 +758,8 @@ def main():
         return adjoint_arm(args)
     if args.decompose:
         return slab_arm(args)
+    if world > 1 and args.scale_mode == "split":
+        return split_arm(args)
     return engine_arm(args)
 
 

@@ -414,8 +414,21 @@ FDTD_B200_API int fdtd_b200_slab_set_source(FdtdB200Slab* h, int cell, const flo
 FDTD_B200_API int fdtd_b200_slab_set_receivers(FdtdB200Slab* h, int n_rec, const int* idx8,
                                                const float* wgt8, int capacity);
 FDTD_B200_API int fdtd_b200_slab_deposit(FdtdB200Slab* h, int n);
+/* Deposit amp (from the host) into this slab's copy of a cell, global flat
+ * index; a no-op when the slab holds no copy of the cell. */
+FDTD_B200_API int fdtd_b200_slab_add_pressure(FdtdB200Slab* h, int cell, float amp);
+/* Read back the receiver samples of the last recorded step (n = the slab's
+ * receiver count); waits for the slab's stream. */
+FDTD_B200_API int fdtd_b200_slab_read_last(FdtdB200Slab* h, float* out, int n);
 /* Fused single-pass step of the own planes (flips both current indices). */
 FDTD_B200_API int fdtd_b200_slab_step(FdtdB200Slab* h);
+/* The same step in two parts, so that the ghost exchange overlaps the
+ * interior: part 1 = the first and last three own planes (what the
+ * neighbours keep as ghosts), part 2 = the planes between them, then the
+ * buffer flip.  Bit-identical to fdtd_b200_slab_step; part 2 may be launched
+ * on another stream (fdtd_b200_slab_set_stream) while part 1's planes are
+ * sent. */
+FDTD_B200_API int fdtd_b200_slab_step_part(FdtdB200Slab* h, int part);
 /* The fused step can also write the neighbours' ghost planes itself (3 planes
  * of the new P, 2 of the new Vx per side), so that only a barrier separates
  * the steps: side 0 = left, 1 = right; fields = the neighbour's eight fields

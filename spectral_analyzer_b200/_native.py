@@ -106,11 +106,14 @@ SIGNATURES = {
     "fdtd_b200_slab_current": (i32, [vp]),
     "fdtd_b200_slab_vset": (i32, [vp]),
     "fdtd_b200_slab_step": (i32, [vp]),
+    "fdtd_b200_slab_step_part": (i32, [vp, i32]),
     "fdtd_b200_slab_set_peer": (i32, [vp, i32, C.POINTER(vp), i32, i32]),
     "fdtd_b200_slab_launch_count": (C.c_longlong, [vp]),
     "fdtd_b200_slab_set_source": (i32, [vp, i32, P_f32, i32]),
     "fdtd_b200_slab_set_receivers": (i32, [vp, i32, P_i32, P_f32, i32]),
     "fdtd_b200_slab_deposit": (i32, [vp, i32]),
+    "fdtd_b200_slab_add_pressure": (i32, [vp, i32, f32]),
+    "fdtd_b200_slab_read_last": (i32, [vp, P_f32, i32]),
     "fdtd_b200_slab_velocity": (i32, [vp]),
     "fdtd_b200_slab_pressure": (i32, [vp]),
     "fdtd_b200_slab_record": (i32, [vp]),

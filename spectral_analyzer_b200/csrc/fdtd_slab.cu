@@ -130,6 +130,12 @@ __global__ void k_slab_deposit(float* p, long long src, const float* __restrict_
     if (s != 0.0f) p[src] = fadd(p[src], s);
 }
 
+// The same deposit with the amplitude passed by the host.
+__global__ void k_slab_add(float* p, long long src, float amp)
+{
+    if (amp != 0.0f) p[src] = fadd(p[src], amp);
+}
+
 // Stability sample (acoustic_fdtd.cpp:1245-1268) over the own cells: global
 // flat indices phase + 1013 t inside [q_lo, q_hi); records the smallest bad one.
 __global__ void k_slab_check(Slab s, const float* __restrict__ p, long long q_first, long long q_hi,
@@ -379,6 +385,32 @@ int fdtd_b200_slab_deposit(FdtdB200Slab* h, int n)
     return FDTD_OK;
 }
 
+// Deposit amp into the local copy of a cell (global flat index; an own or a
+// ghost copy; a no-op when the slab holds no copy of it).
+int fdtd_b200_slab_add_pressure(FdtdB200Slab* h, int cell, float amp)
+{
+    if (!h) return FDTD_ERR_NULL;
+    const long long li = slab_index(h, cell);
+    if (li < 0) return FDTD_OK;
+    k_slab_add<<<1, 1, 0, h->stream>>>(h->P[h->cur], li, amp);
+    ++h->launches;
+    SCK(cudaGetLastError());
+    return FDTD_OK;
+}
+
+// The receiver samples of the last recorded step into out[0 .. n_rec), once
+// the slab's stream has reached them.
+int fdtd_b200_slab_read_last(FdtdB200Slab* h, float* out, int n)
+{
+    if (!h || (!out && n > 0)) return FDTD_ERR_NULL;
+    if (n != h->n_rec) return FDTD_ERR_DIM;
+    if (h->n_rec <= 0 || h->rows == 0) return FDTD_OK;
+    SCK(cudaMemcpyAsync(out, h->d_trace + (size_t)(h->rows - 1) * h->n_rec, sizeof(float) * h->n_rec,
+                        cudaMemcpyDeviceToHost, h->stream));
+    SCK(cudaStreamSynchronize(h->stream));
+    return FDTD_OK;
+}
+
 int fdtd_b200_slab_velocity(FdtdB200Slab* h)
 {
     if (!h) return FDTD_ERR_NULL;
@@ -460,6 +492,54 @@ int fdtd_b200_slab_step(FdtdB200Slab* h)
     }
     SCK(launch_fused_step(a, h->fcache, h->stream));
     ++h->launches;
+    h->cur ^= 1;
+    h->cv ^= 1;
+    return FDTD_OK;
+}
+
+// own planes at each end of a slab that a neighbour keeps as ghosts
+constexpr int GHOST_PLANES = 3;
+
+// The fused step in two launches, so that the ghost exchange can overlap the
+// interior: part 1 computes the own planes a neighbour keeps as ghosts (the
+// first and the last three; the whole slab when it has six planes or fewer),
+// part 2 the planes between them and then flips the buffers.  Both parts
+// read only the old fields and write only their own planes of the new ones,
+// so together they equal fdtd_b200_slab_step bit for bit; part 2 may run on
+// another stream than part 1 (fdtd_b200_slab_set_stream before each call).
+int fdtd_b200_slab_step_part(FdtdB200Slab* h, int part)
+{
+    if (!h) return FDTD_ERR_NULL;
+    if (part != 1 && part != 2) return FDTD_ERR_ARG;
+    if (!fused_supported(h->s.g)) return FDTD_ERR_DIM;
+    if (!h->fcache) h->fcache = fused_cache_create();
+    if (!h->fcache) return FDTD_ERR_CUDA;
+    if (!h->d_status) {
+        SCK(cudaMalloc(&h->d_status, kStatusWords * sizeof(unsigned)));
+        SCK(cudaMemsetAsync(h->d_status, 0xFF, kStatusWords * sizeof(unsigned), h->stream));
+    }
+    float* const* vi = h->V[h->cv];
+    float* const* vo = h->V[h->cv ^ 1];
+    FusedArgs a{h->s.g, h->cf, h->tb, h->P[h->cur], h->P[h->cur ^ 1], {vi[0], vi[1], vi[2]},
+                {vo[0], vo[1], vo[2]}, h->d_status, XSpan{h->s.x0, h->s.nxg, h->s.own_lo, 0}};
+    const int own = h->i1 - h->i0, lo = h->s.own_lo;
+    auto run = [&](int from, int n) -> cudaError_t {
+        if (n <= 0) return cudaSuccess;
+        a.xs.i_lo = from;
+        a.xs.n_own = n;
+        ++h->launches;
+        return launch_fused_step(a, h->fcache, h->stream);
+    };
+    if (part == 1) {
+        if (own <= 2 * GHOST_PLANES) {
+            SCK(run(lo, own));
+        } else {
+            SCK(run(lo, GHOST_PLANES));
+            SCK(run(lo + own - GHOST_PLANES, GHOST_PLANES));
+        }
+        return FDTD_OK;
+    }
+    if (own > 2 * GHOST_PLANES) SCK(run(lo + GHOST_PLANES, own - 2 * GHOST_PLANES));
     h->cur ^= 1;
     h->cv ^= 1;
     return FDTD_OK;

@@ -133,6 +133,20 @@ class EngineSlab:
     def step(self):
         self._check(self._lib.fdtd_b200_slab_step(self._h), "slab_step")
 
+    def add_pressure(self, cell: int, amp: float):
+        """Deposit a host value into this slab's copy of a cell (if it has one)."""
+        self._check(self._lib.fdtd_b200_slab_add_pressure(self._h, int(cell), float(amp)), "slab_add_pressure")
+
+    def read_last(self, out: np.ndarray):
+        """The last recorded step's samples of this slab's receivers, into out."""
+        self._check(self._lib.fdtd_b200_slab_read_last(self._h, out.ctypes.data_as(self._native.P_f32),
+                                                       out.size), "slab_read_last")
+
+    def step_part(self, part: int):
+        """Part 1: the own planes the neighbours keep as ghosts; part 2: the
+        rest, then the buffer flip (together: one step)."""
+        self._check(self._lib.fdtd_b200_slab_step_part(self._h, int(part)), "slab_step_part")
+
     def set_peer(self, side: int, fields, i0: int, i1: int):
         """Let the fused step write the neighbour's ghost planes: fields = its
         eight tensors (or None to clear), [i0, i1) = its planes."""
@@ -250,20 +264,52 @@ class DistExchange:
 
 
 class SlabRunner:
-    """Steps the slabs of one room in lockstep with their ghost exchanges."""
+    """Steps the slabs of one room in lockstep with their ghost exchanges.
 
-    def __init__(self, slabs, exchange):
+    overlap (fused schedule with an exchange): each step computes the planes
+    the neighbours keep as ghosts first, then sends them on a side stream
+    while the interior planes are computed on the slabs' stream; the next
+    step's kernels wait for the exchange."""
+
+    def __init__(self, slabs, exchange, overlap: bool = False):
         self.slabs = list(slabs)
         self.ex = exchange
         self.fused = all(getattr(s, "fused", False) for s in self.slabs)
+        self.overlap = bool(overlap) and self.fused and not isinstance(exchange, PeerStores)
         self.step_count = 0
         self.phase = 0
+        if self.overlap:
+            import torch
+            dev = self.slabs[0].device
+            self._main = torch.cuda.current_stream(dev)
+            self._side = torch.cuda.Stream(dev)
 
-    def step(self, n_steps: int = 1):
+    def _fused_overlapped(self):
+        import torch
+        for s in self.slabs:
+            s.step_part(1)
+        ready = torch.cuda.Event()
+        ready.record(self._main)
+        for s in self.slabs:
+            s.step_part(2)                  # interior on the main stream; flips the buffers
+        with torch.cuda.stream(self._side):
+            self._side.wait_event(ready)
+            self.ex.exchange("P", "Vx")     # the new ghost planes, beside the interior
+        self._main.wait_stream(self._side)
+
+    def step(self, n_steps: int = 1, host_sample=None):
+        """n_steps steps; host_sample(n) -> the source amplitude of step n given
+        by the host (deposited as a launch argument) instead of the slabs'
+        device copy of the signal."""
         for _ in range(int(n_steps)):
             for s in self.slabs:
-                s.deposit(self.step_count)
-            if self.fused:
+                if host_sample is None:
+                    s.deposit(self.step_count)
+                else:
+                    s.add_pressure(s.room.src_flat, host_sample(self.step_count))
+            if self.fused and self.overlap:
+                self._fused_overlapped()
+            elif self.fused:
                 for s in self.slabs:
                     s.step()
                 self.ex.exchange("P", "Vx")
@@ -339,9 +385,11 @@ class PeerDistExchange(DistExchange):
             dist.barrier(group=self.group)
 
 
-def local_room(room: Room, n_slabs: int, device=None, fused: bool = True, peer_stores: bool = False) -> SlabRunner:
+def local_room(room: Room, n_slabs: int, device=None, fused: bool = True, peer_stores: bool = False,
+               overlap: bool = False) -> SlabRunner:
     """All slabs of a room in this process on one GPU (tests, single-GPU runs);
-    peer_stores: the fused steps write each other's ghost planes directly."""
+    peer_stores: the fused steps write each other's ghost planes directly;
+    overlap: plane copies on a side stream beside the interior planes."""
     ranges = partition(room.nx, n_slabs)
     owners = receiver_owner(room, ranges)
     slabs = [EngineSlab(room, a, b, [q for q, o in enumerate(owners) if o == r], device, fused)
@@ -350,15 +398,16 @@ def local_room(room: Room, n_slabs: int, device=None, fused: bool = True, peer_s
         if not fused:
             raise ValueError("peer stores come with the fused step")
         return SlabRunner(slabs, PeerStores(slabs))
-    return SlabRunner(slabs, LocalExchange(slabs))
+    return SlabRunner(slabs, LocalExchange(slabs), overlap=overlap)
 
 
 def distributed_room(room: Room, rank: int, world: int, group=None, device=None,
-                     fused: bool = True, peer_memory: bool = False) -> SlabRunner:
+                     fused: bool = True, peer_memory: bool = False, overlap: bool = False) -> SlabRunner:
     """This rank's slab of a room split over `world` ranks (torch.distributed
     initialised); peer_memory: the fused step writes the neighbours' ghost
     planes through CUDA IPC mappings of their fields and steps end with a
-    barrier (the ranks' GPUs must reach each other's memory)."""
+    barrier (the ranks' GPUs must reach each other's memory); overlap: the
+    exchange runs on a side stream beside the interior planes."""
     ranges = partition(room.nx, world)
     owners = receiver_owner(room, ranges)
     a, b = ranges[rank]
@@ -367,4 +416,4 @@ def distributed_room(room: Room, rank: int, world: int, group=None, device=None,
         if not fused:
             raise ValueError("peer stores come with the fused step")
         return SlabRunner([slab], PeerDistExchange(slab, rank, world, group))
-    return SlabRunner([slab], DistExchange(slab, rank, world, group))
+    return SlabRunner([slab], DistExchange(slab, rank, world, group), overlap=overlap)

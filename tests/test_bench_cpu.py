@@ -1,6 +1,6 @@
-"""The reference arm of bench.py (the reference's CPU solver, no GPU): its JSON
-line carries the fields the benchmark contract asks for, and ranks other than
-0 exit without work."""
+"""bench.py without a GPU: the reference arm (the reference's CPU solver) prints
+the fields the benchmark contract asks for and ranks other than 0 exit without
+work; `--gpus N` launches its ranks itself and reports a split-room line."""
 import json
 import os
 import subprocess
@@ -35,3 +35,22 @@ def test_reference_arm_other_ranks_exit_quietly():
     r = run_bench({"RANK": "1", "WORLD_SIZE": "2"}, "--steps", "1", "--warmup", "3")
     assert r.returncode == 0
     assert not [l for l in r.stdout.splitlines() if l.startswith("{")]
+
+
+def test_bench_launches_its_ranks_and_reports_a_split_run():
+    """`bench.py --gpus 2` without a launcher starts two ranks itself; the
+    plumbing check (gloo, a host stand-in for the step) prints rank 0's line
+    with the split-room keys, and the other rank prints nothing."""
+    import json
+    import subprocess
+    import sys
+    res = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--gpus", "2", "--plumbing-check",
+                          "--steps", "3", "--warmup", "0"], capture_output=True, text=True, timeout=300,
+                         env=dict(os.environ, MASTER_ADDR="127.0.0.1"))
+    assert res.returncode == 0, res.stderr[-2000:]
+    lines = [l for l in res.stdout.splitlines() if l.startswith("{")]
+    assert len(lines) == 1, res.stdout
+    line = json.loads(lines[0])
+    assert line["n_gpus"] == 2 and line["scaling"] == "strong" and line["plumbing_check"]
+    assert line["config"]["parallelism"] == "slab2"
+    assert line["metric"] == "Gcell-updates/s" and line["steps"] == 3

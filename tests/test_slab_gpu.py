@@ -47,15 +47,32 @@ def test_slabs_equal_whole_room(cuda, n_slabs, fused, peer):
     assert all(s.launch_count > 0 for s in run.slabs)
 
 
+@pytest.mark.parametrize("n_slabs", [1, 2, 5, 7])
+def test_overlapped_exchange_equals_whole_room(cuda, n_slabs):
+    """The step in two parts (ghost planes first, then the interior beside the
+    exchange on a side stream) equals the whole room bit for bit; with 7 slabs
+    of 41 planes every slab has six planes or fewer (part 1 covers it all)."""
+    from spectral_analyzer_b200.slab import local_room
+    room = edge_room()
+    tr, P = whole(room)
+    run = local_room(room, n_slabs, overlap=True)
+    assert run.overlap
+    run.step(room.n_steps)
+    got = run.traces(len(room.receivers))
+    assert bits_equal(got, tr), first_mismatch(got, tr)
+    assert bits_equal(run.pressure_field(), P)
+
+
 @pytest.mark.parametrize("fused", [True, False])
 def test_seeded_room_over_four_slabs(cuda, fused):
     from spectral_analyzer_b200.slab import local_room
     room = seeded_room(96, 64, 80, 300, seed=21, n_rec=6, n_pml=8)
     tr, P = whole(room)
-    run = local_room(room, 4, fused=fused)
-    run.step(room.n_steps)
-    assert bits_equal(run.traces(6), tr)
-    assert bits_equal(run.pressure_field(), P)
+    for overlap in ((False, True) if fused else (False,)):
+        run = local_room(room, 4, fused=fused, overlap=overlap)
+        run.step(room.n_steps)
+        assert bits_equal(run.traces(6), tr), overlap
+        assert bits_equal(run.pressure_field(), P), overlap
 
 
 def test_slab_instability(cuda):
