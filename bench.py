@@ -80,6 +80,11 @@ def parse_args():
     ap.add_argument("--scale-mode", choices=["split", "replicas"], default="split",
                     help="N>1: split the room into N slabs along i (strong scaling, one ghost exchange "
                          "per step overlapped with the interior) or run N independent replicas (weak)")
+    ap.add_argument("--amr", action="store_true",
+                    help="the AMR pressure backend on a box grid of --amr-cells^3 cells (gradient order 2, "
+                         "anechoic border): cell-updates/s and bytes moved per cell-step")
+    ap.add_argument("--amr-cells", type=int, default=160)
+    ap.add_argument("--amr-order", type=int, default=2)
     ap.add_argument("--plumbing-check", action="store_true",
                     help="no GPU: ranks on gloo with a host stand-in for the step, to check the "
                          "rank launch, the max-over-ranks timing and the JSON line")
@@ -609,6 +614,77 @@ def slab_arm(args):
     return 0
 
 
+def box_amr_grid(n: int, dx: float = 0.01, n_pml: int = 8):
+    """A box of n^3 cells in the AMR solver's explicit cell/face form (cells in
+    i-major order, faces x then y then z), the outer n_pml layers marked as
+    PML cells (type 3); the layout a uniform region of an AMR grid has."""
+    idx = np.arange(n ** 3, dtype=np.int64).reshape(n, n, n)
+    ax = np.arange(n)
+    I, J, K = np.meshgrid(ax, ax, ax, indexing="ij")
+    centers = np.stack([(I + 0.5) * dx, (J + 0.5) * dx, (K + 0.5) * dx], axis=-1).reshape(-1, 3)
+    edge = np.minimum.reduce([I, J, K, n - 1 - I, n - 1 - J, n - 1 - K]).ravel()
+    types = np.where(edge < n_pml, 3, 0).astype(np.uint8)
+    neg = np.concatenate([idx[:-1].ravel(), idx[:, :-1].ravel(), idx[:, :, :-1].ravel()]).astype(np.int32)
+    pos = np.concatenate([idx[1:].ravel(), idx[:, 1:].ravel(), idx[:, :, 1:].ravel()]).astype(np.int32)
+    nf = neg.size
+    return {"cell_centers": centers, "cell_volumes": np.full(n ** 3, dx ** 3), "open_volume_frac": np.ones(n ** 3),
+            "cell_types": types, "face_cell_neg": neg, "face_cell_pos": pos, "face_area": np.full(nf, dx * dx),
+            "face_open_frac": np.ones(nf), "face_distance": np.full(nf, dx), "min_dx": dx,
+            "bounds_min": np.zeros(3), "bounds_max": np.full(3, n * dx), "n_pml": n_pml}
+
+
+def amr_arm(args):
+    """AMR pressure backend throughput on a box grid (uniform region of an AMR
+    grid): cell-updates/s over the step kernels (velocity + pressure; no plate),
+    with the bytes one step moves per cell in this layout."""
+    import torch
+    from spectral_analyzer_b200.amr import AcousticAMR
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    g = box_amr_grid(args.amr_cells)
+    s = AcousticAMR(g["cell_centers"], g["cell_volumes"], g["open_volume_frac"], g["cell_types"],
+                    g["face_cell_neg"], g["face_cell_pos"], g["face_area"], g["face_open_frac"],
+                    g["face_distance"], 343.0, 1.21, g["min_dx"], args.amr_order)
+    assert s.set_border_condition(0, 3.0, 0.0, 0.0, g["n_pml"], g["bounds_min"], g["bounds_max"]) == 0
+    s.inject_pressure_nearest(g["cell_centers"][len(g["cell_centers"]) // 2], 1.0)
+    s.step_async(args.warmup)
+    assert s.synchronize() == 0
+    s.profile(True)
+    l0 = s.launch_count
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s.step_async(args.steps)
+    rc = s.synchronize()
+    wall = time.perf_counter() - t0
+    ms, n = s.profile_read()
+    assert rc == 0 and n == args.steps
+    nc, nf = s.n_cells, s.n_faces
+    entries = 2 * nf
+    # algorithmic bytes per step, every array element touched once per kernel:
+    # velocity: v in/out, V_damp, the gradient's operands (neg, pos, 1/d; or the
+    #           8-slot stencil's cells and weights) per face, p once per cell;
+    # pressure: p in/out, P_damp, P_src, 1/(V open), wall flag, CSR start per
+    #           cell, CSR face and weight per entry, v once per face
+    grad = (4 + 4 + 4) if args.amr_order == 2 else 8 * (4 + 4)
+    face_b = nf * (4 + 4 + 4 + grad) + nf * 4
+    cell_b = nc * 4 + nc * (4 + 4 + 4 + 4 + 4 + 1 + 4) + entries * (4 + 4)
+    step_ms = ms / n
+    peak, peak_kind = measured_peak()
+    gbs = (face_b + cell_b) / (step_ms / 1e3) / 1e9
+    line = {"metric": "AMR cell-updates/s", "value": nc / (step_ms / 1e3) / 1e9, "unit": "Gcell-updates/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms,
+            "wall_ms_per_step": wall / args.steps * 1e3, "higher_is_better": True, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"amr_box{args.amr_cells}^3_order{args.amr_order}", "cells": nc, "faces": nf,
+                       "border": "anechoic, 8 PML cells", "kernels": "k_amr_velocity + k_amr_pressure"},
+            "roofline": {"bound": "hbm", "achieved": gbs, "peak": peak, "unit": "GB/s", "frac": gbs / peak,
+                         "peak_kind": f"{peak_kind} hbm_gbs", "bytes_per_step": face_b + cell_b,
+                         "bytes_per_cell_step": (face_b + cell_b) / nc},
+            "gpu_launches": s.launch_count - l0}
+    print(json.dumps(line), flush=True)
+    s.close()
+    return 0
+
+
 def launch_ranks(n: int, argv) -> int:
     """Re-run this script as n ranks (torch.distributed.run, one GPU each) when
     it was started without a launcher; returns the launcher's exit code."""
@@ -758,6 +834,8 @@ def main():
         return adjoint_arm(args)
     if args.decompose:
         return slab_arm(args)
+    if args.amr:
+        return amr_arm(args)
     if world > 1 and args.scale_mode == "split":
         return split_arm(args)
     return engine_arm(args)
