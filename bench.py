@@ -680,8 +680,25 @@ def amr_arm(args):
                          "peak_kind": f"{peak_kind} hbm_gbs", "bytes_per_step": face_b + cell_b,
                          "bytes_per_cell_step": (face_b + cell_b) / nc},
             "gpu_launches": s.launch_count - l0}
-    print(json.dumps(line), flush=True)
     s.close()
+    if not args.no_cpu_baseline:
+        # the reference's own AMR stepper (oracle/_ref/libamr_ref.so, its thread pool) on the same grid
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        from amr_oracle import AMRRef
+        g["n_cells"], g["n_faces"], g["c"], g["rho_air"] = nc, nf, 343.0, 1.21
+        r = AMRRef(g, gradient_order=args.amr_order, border=(0, 3.0, 0.0, 0.0))
+        r.step_rc(1)
+        n_cpu, t0 = 0, time.perf_counter()
+        while time.perf_counter() - t0 < args.cpu_seconds and n_cpu < 2000:
+            assert r.step_rc(1) == 0
+            n_cpu += 1
+        el = time.perf_counter() - t0
+        r.close()
+        line["cpu_baseline"] = {"value": nc * n_cpu / el / 1e9, "unit": "Gcell-updates/s",
+                                "cores": os.cpu_count(), "kind": "reference",
+                                "sample": f"{n_cpu} steps of the same grid ({el:.1f} s wall, libamr_ref.so, "
+                                          "its thread pool over all host cores)"}
+    print(json.dumps(line), flush=True)
     return 0
 
 

@@ -86,6 +86,14 @@ class AMRRef:
         if not h:
             raise RuntimeError("amr_create failed: " + (lib.amr_get_last_create_error_message() or b"").decode())
         self._h = C.c_void_p(h)
+        if "plate_Nx" not in d:           # a grid without a plate (no sources either)
+            self._plate_nodes = 0
+            if int(d.get("n_pml", 0)) > 0 and border is not None:
+                mode, sig, R, Z = border
+                rc = lib.amr_set_border_condition(self._h, int(mode), float(sig), float(R), float(Z),
+                                                  int(d["n_pml"]), _p(d["bounds_min"]), _p(d["bounds_max"]))
+                assert rc == 0, rc
+            return
         self._plate_nodes = int(d["plate_Nx"]) * int(d["plate_Ny"])
         rc = lib.amr_setup_plate(
             self._h, int(d["plate_Nx"]), int(d["plate_Ny"]), float(d["plate_dx"]), _p(d["plate_origin"]),

@@ -202,6 +202,7 @@ int build_tables(AcousticFDTDState* st)
         float denom = 1.0f + ax[q] * dt;
         px[q] = 1.0f / denom;
     }
+    x_interior_run(ax, nx, &st->tb.xi_lo, &st->tb.xi_hi);
     CK(cudaMemcpyAsync(st->d_tab, h.data(), h.size() * sizeof(float), cudaMemcpyHostToDevice,
                        st->stream));
     CK(cudaStreamSynchronize(st->stream));

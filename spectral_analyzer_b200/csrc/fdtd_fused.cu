@@ -43,6 +43,7 @@
 #include <cudaTypedefs.h>
 
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 namespace fdtd {
@@ -400,7 +401,26 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
     float axw3 = ax_at(u0 - 3), axw2 = ax_at(u0 - 2), axw1 = ax_at(u0 - 1), axw0 = ax_at(u0);
     float pxw = px_at(u0 - 3);
 
-    for (int u = u0; u <= u1; ++u) {
+    // The interior iterations of a clean tile take a separately compiled body
+    // without the general path (a general path present in the loop costs the
+    // interior about 12 % although it never runs there).  Iteration u is
+    // interior when plane u-3 and faces u-2 .. u-1 have no x absorption, face
+    // u-2 has the 4th-order gradient and the planes u-3, u-2 are own ones; a
+    // tile is clean when every row of its Vy faces has the 4th-order gradient
+    // and all its columns are cells.  Both bodies evaluate the same expressions
+    // (alpha_x = 0, px = 1 there), so the results do not depend on the choice.
+    const bool clean = kfull && j0 - 2 >= 1 && j0 + C::TJ <= ny - 3;
+    int fast_lo = u1 + 1, fast_hi = u1 + 1;
+    if (clean && a.tb.xi_hi > a.tb.xi_lo) {
+        fast_lo = max(max(a.tb.xi_lo + 3, 3 - xg0), i_beg + 3);
+        fast_hi = min(min(a.tb.xi_hi + 1, nxg - xg0), u1 + 1);
+        if (fast_lo >= fast_hi) fast_lo = fast_hi = u1 + 1;
+    }
+
+    // One iteration of the march; FAST = the interior body.  False when a load
+    // wait ran out (u_fail is then set).
+    auto iteration = [&](const int u, auto fast_tag) -> bool {
+        constexpr bool FAST = decltype(fast_tag)::value;
         // wait for plane u (P) and iteration u's V data; the decision to stop on a
         // timeout is made by the whole CTA (the barrier below is also the one that
         // separates the previous iteration's reads from this iteration's writes)
@@ -419,7 +439,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicMin(a.status + kStatusTimeout, blockIdx.x + gridDim.x * blockIdx.y);
             u_fail = u;
-            break;
+            return false;
         }
         pph ^= 1u << ps;
         vph ^= 1u << vsg;
@@ -427,35 +447,43 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
         // reads came before the barrier above), so thread 0 issues them before
         // its own work of this iteration rather than after it
         if (tid == 0 && u + C::D <= u1) issue(u + C::D, pslot[C::RING - 1], vslot[C::VSTAGES - 1]);
-        const float ax_next = ax_at(u + 1), px_next = px_at(u - 2);
+        float ax_next = 0.0f, px_next = 1.0f;
+        if constexpr (!FAST) {
+            ax_next = ax_at(u + 1);
+            px_next = px_at(u - 2);
+        }
         const float* vs = smem + C::VST0 + vsg * C::V_STAGE;
 
         // ---- new Vx on face f = u-2 of the own columns (planes f-1 .. f+2) ----
-        if (u >= i_beg) {
+        if (FAST || u >= i_beg) {
             const int f = u - 2, fg = f + xg0;
             float4 vnew = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (fg >= 0 && fg <= nxg - 2 && row_ok) {
-                const bool fourth = (fg > 0 && fg < nxg - 2);
-                const float axf = axw2, axf1 = axw1;     // alpha_x[f], alpha_x[f+1]
+            if (FAST || (fg >= 0 && fg <= nxg - 2 && row_ok)) {
                 const float4 pm = lds4(smem + C::RING0 + pslot[0] * C::P_STAGE + cP);
                 const float4 p0 = lds4(smem + C::RING0 + pslot[1] * C::P_STAGE + cP);
                 const float4 p1 = lds4(smem + C::RING0 + pslot[2] * C::P_STAGE + cP);
                 const float4 p2 = lds4(smem + C::RING0 + pslot[3] * C::P_STAGE + cP);
                 const float4 vo = lds4(vs + C::VX_OFF + 4 * tid);
-                if (fourth && axf == 0.0f && axf1 == 0.0f && kfull) {
+                if constexpr (FAST) {
                     vnew = vel4(cf, pm, p0, p1, p2, vo, dxi);
                 } else {
-                    float4 aL, aR;
-                    int okx = 0;
+                    const bool fourth = (fg > 0 && fg < nxg - 2);
+                    const float axf = axw2, axf1 = axw1;     // alpha_x[f], alpha_x[f+1]
+                    if (fourth && axf == 0.0f && axf1 == 0.0f && kfull) {
+                        vnew = vel4(cf, pm, p0, p1, p2, vo, dxi);
+                    } else {
+                        float4 aL, aR;
+                        int okx = 0;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        at(aL, q) = fmaxf(axf, at(myz, q));
-                        at(aR, q) = fmaxf(axf1, at(myz, q));
-                        okx |= (kb + q < nz) ? (1 << q) : 0;
+                        for (int q = 0; q < 4; ++q) {
+                            at(aL, q) = fmaxf(axf, at(myz, q));
+                            at(aR, q) = fmaxf(axf1, at(myz, q));
+                            okx |= (kb + q < nz) ? (1 << q) : 0;
+                        }
+                        vnew = vel4_general(cf, pm, p0, p1, p2, vo, aL, aR, fourth ? 15 : 0, okx);
                     }
-                    vnew = vel4_general(cf, pm, p0, p1, p2, vo, aL, aR, fourth ? 15 : 0, okx);
                 }
-                if (f >= i_beg && f < i_end && st_ok) {
+                if (f >= i_beg && f < i_end && (FAST || st_ok)) {
                     stg4(a.vout[0] + f * PL + own, vnew);
 #pragma unroll
                     for (int sd = 0; sd < 2; ++sd)   // the neighbours' ghost faces
@@ -469,9 +497,9 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
         // ---- plane i = u-3: new Vy / Vz (with halos), then P^{n+1} ----
         {
             const int i = u - 3;
-            if (i >= i_beg) {
-                const float axi = axw3;                  // alpha_x[i]
-                const bool xint = (axi == 0.0f);
+            if (FAST || i >= i_beg) {
+                const float axi = FAST ? 0.0f : axw3;    // alpha_x[i]
+                const bool xint = FAST || (axi == 0.0f);
                 const float* pst = smem + C::RING0 + pslot[0] * C::P_STAGE;
                 const float* vys = vs + C::VY_OFF;
                 const float* vzs = vs + C::VZ_OFF;
@@ -484,27 +512,31 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                     if (r < C::VYR) {
                         const int jf = j0 - 2 + r;
                         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (jf >= 0 && jf <= ny - 2) {
-                            const bool fourth = (jf > 0 && jf < ny - 2);
+                        if (FAST || (jf >= 0 && jf <= ny - 2)) {
                             const float* pc = pst + 4 * lane + 4;
                             const float4 pm = lds4(pc + r * C::PC), p0 = lds4(pc + (r + 1) * C::PC);
                             const float4 p1 = lds4(pc + (r + 2) * C::PC), p2 = lds4(pc + (r + 3) * C::PC);
                             const float4 vo = lds4(vys + r * C::TK + 4 * lane);
-                            if (fourth && xint && kfull) {
+                            if constexpr (FAST) {
                                 v = vel4(cf, pm, p0, p1, p2, vo, dyi[m]);
                             } else {
-                                float4 aL, aR;
-                                int oky = 0;
+                                const bool fourth = (jf > 0 && jf < ny - 2);
+                                if (fourth && xint && kfull) {
+                                    v = vel4(cf, pm, p0, p1, p2, vo, dyi[m]);
+                                } else {
+                                    float4 aL, aR;
+                                    int oky = 0;
 #pragma unroll
-                                for (int q = 0; q < 4; ++q) {
-                                    const float azk = az_s[4 * lane + 4 + q];
-                                    at(aL, q) = fmaxf(fmaxf(axi, ay_s[r]), azk);
-                                    at(aR, q) = fmaxf(fmaxf(axi, ay_s[r + 1]), azk);
-                                    oky |= (kb + q < nz) ? (1 << q) : 0;
+                                    for (int q = 0; q < 4; ++q) {
+                                        const float azk = az_s[4 * lane + 4 + q];
+                                        at(aL, q) = fmaxf(fmaxf(axi, ay_s[r]), azk);
+                                        at(aR, q) = fmaxf(fmaxf(axi, ay_s[r + 1]), azk);
+                                        oky |= (kb + q < nz) ? (1 << q) : 0;
+                                    }
+                                    v = vel4_general(cf, pm, p0, p1, p2, vo, aL, aR, fourth ? 15 : 0, oky);
                                 }
-                                v = vel4_general(cf, pm, p0, p1, p2, vo, aL, aR, fourth ? 15 : 0, oky);
                             }
-                            if (r >= 2 && r < C::TJ + 2 && kb < sz)
+                            if (r >= 2 && r < C::TJ + 2 && (FAST || kb < sz))
                                 stg4(a.vout[1] + ib + (long long)jf * sz + kb, v);
                         }
                         sts4(vyn + r * C::TK + 4 * lane, v);
@@ -516,7 +548,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                 {
                     const float* prow = pst + (w + 3) * C::PC;
                     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (row_ok) {
+                    if (FAST || row_ok) {
                         const int c = 4 * lane + 4;            // col of kb
                         pown = lds4(prow + c);
                         const float4 pb4 = lds4(prow + c + 4);
@@ -538,7 +570,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                             }
                             v = vel4_general(cf, pm, pown, p1, p2, vo, aL, aR, zm4, zok);
                         }
-                        if (st_ok) stg4(a.vout[2] + ib + own, v);
+                        if (FAST || st_ok) stg4(a.vout[2] + ib + own, v);
                     }
                     sts4(vzn + w * C::PC + 4 * lane + 4, v);
                 }
@@ -551,7 +583,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                     const int kf = k0 - 4 + ch;
                     const float* prow = pst + (jl + 3) * C::PC;
                     float vh = 0.0f;
-                    if (j0 + jl < ny && kf >= 0 && kf <= nz - 2) {
+                    if ((FAST || j0 + jl < ny) && kf >= 0 && kf <= nz - 2) {
                         const bool fourth = (kf > 0 && kf < nz - 2);
                         const float ay = ay_s[jl + 2];
                         const float gr = grad4(cf, prow[ch - 1], prow[ch], prow[ch + 1], prow[ch + 2], fourth);
@@ -564,7 +596,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                 __syncthreads();
 
                 // P^{n+1} of the own cells
-                if (row_ok) {
+                if (FAST || row_ok) {
                     const float* yr = vyn + 4 * lane;
                     const float4 ymm = lds4(yr + w * C::TK), ym = lds4(yr + (w + 1) * C::TK);
                     const float4 yp = lds4(yr + (w + 2) * C::TK), ypp = lds4(yr + (w + 3) * C::TK);
@@ -573,18 +605,23 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                     const float4 zb = lds4(zr + 4);                                // faces kb .. kb+3
                     const float zc = zr[8];                                        // face kb+4
                     // px[i] = 1 on x-interior planes, so min(px[i], min(py, pz)) = mpz there
-                    const float pxi = pxw;
+                    float4 pd = mpz;
+                    if constexpr (!FAST) {
+                        const float pxi = pxw;
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) at(pd, q) = fminf(pxi, at(mpz, q));
+                    }
                     float4 out;
-                    out.x = pupd(cf, pown.x, qx2.x, qx1.x, qx3.x, qx0.x, yp.x, ym.x, ypp.x, ymm.x, zb.x, za.y, zb.y, za.x, fminf(pxi, mpz.x));
-                    out.y = pupd(cf, pown.y, qx2.y, qx1.y, qx3.y, qx0.y, yp.y, ym.y, ypp.y, ymm.y, zb.y, zb.x, zb.z, za.y, fminf(pxi, mpz.y));
-                    out.z = pupd(cf, pown.z, qx2.z, qx1.z, qx3.z, qx0.z, yp.z, ym.z, ypp.z, ymm.z, zb.z, zb.y, zb.w, zb.x, fminf(pxi, mpz.z));
-                    out.w = pupd(cf, pown.w, qx2.w, qx1.w, qx3.w, qx0.w, yp.w, ym.w, ypp.w, ymm.w, zb.w, zb.z, zc, zb.y, fminf(pxi, mpz.w));
-                    if (!kfull) {
+                    out.x = pupd(cf, pown.x, qx2.x, qx1.x, qx3.x, qx0.x, yp.x, ym.x, ypp.x, ymm.x, zb.x, za.y, zb.y, za.x, pd.x);
+                    out.y = pupd(cf, pown.y, qx2.y, qx1.y, qx3.y, qx0.y, yp.y, ym.y, ypp.y, ymm.y, zb.y, zb.x, zb.z, za.y, pd.y);
+                    out.z = pupd(cf, pown.z, qx2.z, qx1.z, qx3.z, qx0.z, yp.z, ym.z, ypp.z, ymm.z, zb.z, zb.y, zb.w, zb.x, pd.z);
+                    out.w = pupd(cf, pown.w, qx2.w, qx1.w, qx3.w, qx0.w, yp.w, ym.w, ypp.w, ymm.w, zb.w, zb.z, zc, zb.y, pd.w);
+                    if (!FAST && !kfull) {
 #pragma unroll
                         for (int q = 0; q < 4; ++q)
                             if (kb + q >= nz) at(out, q) = 0.0f;
                     }
-                    if (kb < sz) {
+                    if (FAST || kb < sz) {
                         stg4(a.pn + ib + own, out);
 #pragma unroll
                         for (int sd = 0; sd < 2; ++sd)   // the neighbours' ghost planes
@@ -595,12 +632,11 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
             }
         }
 
-        axw3 = axw2; axw2 = axw1; axw1 = axw0; axw0 = ax_next;
-        pxw = px_next;
+        if constexpr (!FAST) {
+            axw3 = axw2; axw2 = axw1; axw1 = axw0; axw0 = ax_next;
+            pxw = px_next;
+        }
         // rotate: after it pslot[q] holds plane u+1-3+q and vslot[q] iteration u+1+q.
-        // The slots receiving iteration u+D's loads (pslot[3+D-1], vslot[D-1]) were
-        // freed one iteration ago: their last reads (plane u-4, iteration u-1)
-        // happened before this iteration's first barrier.
         {
             const int pfree = pslot[0];
 #pragma unroll
@@ -611,6 +647,22 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
             for (int q = 0; q + 1 < C::VSTAGES; ++q) vslot[q] = vslot[q + 1];
             vslot[C::VSTAGES - 1] = vfree;
         }
+        return true;
+    };
+
+    for (int u = u0; u <= u1;) {
+        if (u == fast_lo) {
+            bool ran = true;
+            for (; u < fast_hi; ++u)
+                if (!iteration(u, std::true_type{})) { ran = false; break; }
+            if (!ran) break;
+            // the window of the general iterations that follow
+            axw3 = ax_at(u - 3); axw2 = ax_at(u - 2); axw1 = ax_at(u - 1); axw0 = ax_at(u);
+            pxw = px_at(u - 3);
+            continue;
+        }
+        if (!iteration(u, std::false_type{})) break;
+        ++u;
     }
 
     // A normal march waits for every load it issued, so none is in flight here.

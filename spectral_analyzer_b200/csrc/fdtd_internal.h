@@ -52,7 +52,26 @@ struct Tables {        // per-axis absorption tables, lengths nx, ny, nz
     const float* px;   // 1/(1 + ax*dt)
     const float* py;
     const float* pz;
+    int xi_lo, xi_hi;  // planes [xi_lo, xi_hi) have ax == 0 (x-interior); empty: none
 };
+
+// The longest run [lo, hi) of planes with alpha_x == 0 (the interior between
+// the x absorbing layers, extended through a layer whose absorption is 0;
+// a slab's ghost planes outside the room also have alpha_x == 0, so the
+// longest run is taken); empty when there is none.
+inline void x_interior_run(const float* ax, int n, int* lo, int* hi)
+{
+    int best_lo = 0, best_hi = 0;
+    for (int a = 0; a < n;) {
+        if (ax[a] != 0.0f) { ++a; continue; }
+        int b = a;
+        while (b < n && ax[b] == 0.0f) ++b;
+        if (b - a > best_hi - best_lo) { best_lo = a; best_hi = b; }
+        a = b;
+    }
+    *lo = best_lo;
+    *hi = best_hi;
+}
 
 struct PlateCoef {
     float a;    // dt^2 / (rho_s h)

@@ -298,6 +298,7 @@ FdtdB200Slab* fdtd_b200_slab_create(int Nx, int Ny, int Nz, int i0, int i1, floa
     h->tb.px = h->d_tab + L + Ny + Nz;
     h->tb.py = h->tb.px + L;
     h->tb.pz = h->tb.py + Ny;
+    x_interior_run(ax, L, &h->tb.xi_lo, &h->tb.xi_hi);
     return h;
 }
 
