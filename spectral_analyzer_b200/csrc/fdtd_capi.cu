@@ -1408,6 +1408,29 @@ int fdtd_b200_device_fields(const AcousticFDTDState* st, void** out5)
     return FDTD_OK;
 }
 
+// The step counter and the stability check's rotating phase: with the
+// current P and V fields they are the whole state a later step depends on
+// (the source schedule and receivers are configuration), so a snapshot of
+// the five fields plus these two resumes a room exactly.
+int fdtd_b200_get_progress(const AcousticFDTDState* st, int* step_count, int* check_phase)
+{
+    if (!st || !step_count || !check_phase) return FDTD_ERR_NULL;
+    *step_count = st->step_count;
+    *check_phase = st->stab_phase;
+    return FDTD_OK;
+}
+
+int fdtd_b200_set_progress(AcousticFDTDState* st, int step_count, int check_phase)
+{
+    if (!st) return FDTD_ERR_NULL;
+    if (step_count < 0 || check_phase < 0 || check_phase >= kCheckStride) return FDTD_ERR_ARG;
+    if (dev_guard(st)) return FDTD_ERR_CUDA;
+    CK(cudaStreamSynchronize(st->stream));
+    st->step_count = step_count;
+    st->stab_phase = check_phase;
+    return FDTD_OK;
+}
+
 int fdtd_b200_profile(AcousticFDTDState* st, int enable)
 {
     if (!st) return FDTD_ERR_NULL;

@@ -189,6 +189,9 @@ class EngineBatch:
 
 
 # ---------------------------------------------------------------- schedulers
+PREEMPTED = "pre-empted"      # a running request taken off the GPU by preempt()
+
+
 class BatchServer:
     """Continuous batching: admit on arrival when a slot and memory are free.
 
@@ -210,11 +213,28 @@ class BatchServer:
         self.sleep = sleep
         self.log: List[dict] = []
         self._cancelled: set = set()
+        self._preempt: set = set()
+        self._resume: set = set()
+        self.paused: Dict[int, tuple] = {}   # rid -> (request, snapshot, traces so far, first start)
 
     def cancel(self, rid: int) -> None:
         """Ask for request ``rid`` to be dropped (queued) or evicted (running)
         at the next scheduling point; safe to call from another thread."""
         self._cancelled.add(rid)
+
+    def preempt(self, rid: int) -> None:
+        """Ask for running request ``rid`` to leave the GPU at the next
+        scheduling point: its state (fields, step count, check phase) and the
+        traces recorded so far go to host memory and its slot and device
+        memory are freed.  It waits until ``resume(rid)``; then it is admitted
+        again before the queued requests and continues exactly where it
+        stopped (the traces of both parts are joined).  Safe to call from
+        another thread."""
+        self._preempt.add(rid)
+
+    def resume(self, rid: int) -> None:
+        """Let a pre-empted request ``rid`` back in (at the next scheduling point)."""
+        self._resume.add(rid)
 
     def run(self, requests: Sequence[Request]) -> List[Result]:
         be = self.backend
@@ -226,6 +246,7 @@ class BatchServer:
         if self.tile_k != 128:
             batch.set_tile(self.tile_k)
         active: List[tuple] = []          # (request, solver, start_time)
+        self._parts: Dict[int, np.ndarray] = {}   # traces recorded before a pre-emption
         used = 0
         results: List[Result] = []
         t0 = self.clock()
@@ -238,8 +259,28 @@ class BatchServer:
         def late(req, now):
             return req.deadline is not None and now > req.arrival + req.deadline
 
-        while queue or active:
+        resumed: deque = deque()          # (request, snapshot, traces so far, first start)
+        while queue or active or resumed or (self.paused and self._resume & set(self.paused)):
             now = self.clock() - t0
+            for rid in list(self._resume):
+                if rid in self.paused:
+                    resumed.append(self.paused.pop(rid))
+                    self._resume.discard(rid)
+            # pre-empted requests come back first, when a slot and memory are free
+            while resumed and room_bytes(resumed[0][0].room) > budget:
+                reject(resumed.popleft()[0], now, "exceeds the memory budget")
+            while resumed and len(active) < self.max_slots and used + room_bytes(resumed[0][0].room) <= budget:
+                req, snap, part, start = resumed.popleft()
+                try:
+                    solver = be.make(req.room)
+                    be.restore(solver, snap)
+                except (RuntimeError, MemoryError) as e:
+                    reject(req, now, f"allocation failed on resume: {e}")
+                    continue
+                self._parts[req.rid] = part
+                active.append((req, solver, start))
+                used += room_bytes(req.room)
+                dirty = True
             # queued requests that were cancelled, ran out of time, or can never fit
             if queue:
                 keep_q = deque()
@@ -267,6 +308,8 @@ class BatchServer:
             if not active:
                 if queue:
                     self.sleep(min(max(queue[0].arrival - now, 0.0), 0.05))
+                elif not resumed:
+                    break                 # only pre-empted requests left, none resumed
                 continue
             if dirty:
                 batch.set([s for _, s, _ in active], [r.room.n_steps for r, _, _ in active])
@@ -284,16 +327,27 @@ class BatchServer:
                     leave[q] = "cancelled"
                 elif late(r, now):
                     leave[q] = "deadline exceeded"
+                elif r.rid in self._preempt:
+                    leave[q] = PREEMPTED
             self.log.append({"t": now, "active": len(active),
                              "finished": sum(1 for e in leave.values() if e is None),
-                             "failed": sum(1 for e in leave.values() if e is not None),
+                             "preempted": sum(1 for e in leave.values() if e is PREEMPTED),
+                             "failed": sum(1 for e in leave.values() if e is not None and e is not PREEMPTED),
                              "queued": len(queue)})
             if leave:
                 keep = [a for q, a in enumerate(active) if q not in leave]
                 batch.set([s for _, s, _ in keep], [r.room.n_steps for r, _, _ in keep])
                 for q, err in leave.items():
                     req, solver, start = active[q]
-                    results.append(Result(req.rid, be.traces(solver), req.arrival, start, now, error=err))
+                    tr = be.traces(solver)
+                    part = self._parts.pop(req.rid, None)
+                    if part is not None:
+                        tr = np.concatenate([part, tr], axis=0)
+                    if err is PREEMPTED:
+                        self._preempt.discard(req.rid)
+                        self.paused[req.rid] = (req, be.snapshot(solver), tr, start)
+                    else:
+                        results.append(Result(req.rid, tr, req.arrival, start, now, error=err))
                     used -= room_bytes(req.room)
                     be.release(solver)
                 active = keep
@@ -351,6 +405,12 @@ class _EngineBackend:
 
     def traces(self, solver) -> np.ndarray:
         return solver.get_traces()
+
+    def snapshot(self, solver) -> dict:
+        return solver.snapshot()
+
+    def restore(self, solver, snap: dict):
+        solver.restore(snap)
 
     def release(self, solver):
         solver.close()

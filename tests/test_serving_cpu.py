@@ -93,7 +93,13 @@ class FakeBackend:
         self.clock.t += 1e-4 * n
 
     def traces(self, solver):
-        return np.arange(solver.step, dtype=np.float32)[:, None]
+        return np.arange(getattr(solver, "start", 0), solver.step, dtype=np.float32)[:, None]
+
+    def snapshot(self, solver):
+        return {"step": solver.step}
+
+    def restore(self, solver, snap):
+        solver.step = solver.start = snap["step"]
 
     def release(self, solver):
         self.live -= 1
@@ -248,3 +254,45 @@ def test_allocation_failure_and_oversized_request_are_rejected():
     assert res[reqs[1].rid].error.startswith("allocation failed")
     assert sum(r.ok for r in res.values()) == 5
     assert be.peak_bytes <= budget
+
+
+def test_preempt_and_resume_continue_where_they_stopped():
+    """A running request pre-empted at a chunk boundary leaves the GPU (slot and
+    memory freed) with its state; resumed, it continues from its step and its
+    result joins both parts, as if it had run without a pause."""
+    clock = FakeClock()
+    be = FakeBackend(clock)
+    reqs = small_requests(6)
+    for r in reqs:
+        r.arrival = 0.0
+        r.room.n_steps = 400
+    srv = BatchServer(max_slots=8, chunk=64, backend=be, clock=clock, sleep=clock.sleep)
+    target = reqs[2].rid
+    srv.preempt(target)
+    first = srv.run(reqs)
+    assert target not in [r.rid for r in first] and target in srv.paused
+    assert srv.log[0]["preempted"] == 1
+    req, snap, part, _ = srv.paused[target]
+    assert snap["step"] == 64 and part.shape == (64, 1)
+    live_before = be.live
+    srv.resume(target)
+    second = srv.run([])
+    assert [r.rid for r in second] == [target] and not srv.paused
+    res = second[0]
+    assert res.ok and np.array_equal(res.traces[:, 0], np.arange(400, dtype=np.float32))
+    assert be.live == live_before                        # every solver released
+    assert all(r.ok and r.traces.shape[0] == 400 for r in first)
+
+
+def test_paused_request_stays_paused_without_resume():
+    clock = FakeClock()
+    be = FakeBackend(clock)
+    reqs = small_requests(3)
+    for r in reqs:
+        r.arrival = 0.0
+    srv = BatchServer(max_slots=4, chunk=32, backend=be, clock=clock, sleep=clock.sleep)
+    srv.preempt(reqs[0].rid)
+    out = srv.run(reqs)
+    assert sorted(r.rid for r in out) == sorted(r.rid for r in reqs[1:])
+    assert list(srv.paused) == [reqs[0].rid]
+    assert srv.run([]) == []                             # nothing to do until resume

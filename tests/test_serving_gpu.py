@@ -184,3 +184,44 @@ def test_server_isolates_a_diverging_request(cuda):
     for q in (0, 1, 3):
         assert res[q].ok
         assert bits_equal(res[q].traces, alone(rs[q])[0])
+
+
+def test_preempted_request_resumes_bit_exact(cuda):
+    """Two requests of the mix are pre-empted after their first chunk (their
+    fields, step count and check phase go to host memory and their slots are
+    freed), the others finish, then both resume on new solvers: every result
+    equals the room run alone, bit for bit.  One of them crosses a 256-step
+    check after the resume."""
+    from spectral_analyzer_b200.serving import BatchServer, Request
+    rs = rooms()
+    ref = [alone(r) for r in rs]
+    reqs = [Request(q, r, 0.0) for q, r in enumerate(rs)]
+    srv = BatchServer(max_slots=8, chunk=64)
+    srv.preempt(1)
+    srv.preempt(4)
+    first = srv.run(reqs)
+    assert sorted(srv.paused) == [1, 4]
+    assert sorted(r.rid for r in first) == [0, 2, 3, 5]
+    srv.resume(1)
+    srv.resume(4)
+    second = srv.run([])
+    res = {r.rid: r for r in first + second}
+    for q, r in enumerate(rs):
+        assert res[q].ok, res[q].error
+        assert bits_equal(res[q].traces, ref[q][0]), (q, first_mismatch(res[q].traces, ref[q][0]))
+
+
+def test_snapshot_restores_fields_and_progress(cuda):
+    from spectral_analyzer_b200.serving import make_solver
+    room = rooms()[1]
+    a = make_solver(room)
+    a.step(100)
+    snap = a.snapshot()
+    assert snap["step"] == 100
+    b = make_solver(room)
+    b.restore(snap)
+    a.step(room.n_steps - 100)
+    b.step(room.n_steps - 100)
+    assert bits_equal(a.get_pressure_field(), b.get_pressure_field())
+    assert bits_equal(a.get_velocity_x(), b.get_velocity_x())
+    assert b.step_count == room.n_steps
