@@ -242,13 +242,17 @@ FDTD_B200_API int fdtd_b200_debug_hold_load(AcousticFDTDState* st, int plane, in
 /* Device pointers of the current fields: out5 = {P (current), P (next), Vx, Vy, Vz}. */
 FDTD_B200_API int fdtd_b200_device_fields(const AcousticFDTDState* st, void** out5);
 
-/* Progress of a room: its step count and the rotating phase of the 256-step
- * stability check.  With the current fields (fdtd_b200_device_fields) they are
- * the state a later step depends on: copying the fields into another handle
- * of the same room and setting its progress resumes the room exactly (a
- * serving pre-emption snapshot). */
-FDTD_B200_API int fdtd_b200_get_progress(const AcousticFDTDState* st, int* step_count, int* check_phase);
-FDTD_B200_API int fdtd_b200_set_progress(AcousticFDTDState* st, int step_count, int check_phase);
+/* Progress of a room: its step count, the rotating phase of the 256-step
+ * stability check, and the step whose source sample is already in P (-1:
+ * none; a batch deposits the next step's sample ahead of it).  With the
+ * current fields (fdtd_b200_device_fields) they are the state a later step
+ * depends on: copying the fields into another handle of the same room and
+ * setting its progress resumes the room exactly (a serving pre-emption
+ * snapshot). */
+FDTD_B200_API int fdtd_b200_get_progress(const AcousticFDTDState* st, int* step_count, int* check_phase,
+                                         int* deposited_step);
+FDTD_B200_API int fdtd_b200_set_progress(AcousticFDTDState* st, int step_count, int check_phase,
+                                         int deposited_step);
 
 /* CUDA-event timing of the main step kernel(s) on the handle's stream. */
 FDTD_B200_API int fdtd_b200_profile(AcousticFDTDState* st, int enable);

@@ -120,8 +120,8 @@ SIGNATURES = {
     "fdtd_b200_slab_check": (i32, [vp, i32, C.POINTER(C.c_longlong)]),
     "fdtd_b200_slab_get_traces": (i32, [vp, P_f32, i32, P_i32]),
     "fdtd_b200_substep": (i32, [vp, P_f32, f32, i32, P_i32, P_f32, f32, i32, P_i32, P_f32, P_f32]),
-    "fdtd_b200_get_progress": (i32, [vp, P_i32, P_i32]),
-    "fdtd_b200_set_progress": (i32, [vp, i32, i32]),
+    "fdtd_b200_get_progress": (i32, [vp, P_i32, P_i32, P_i32]),
+    "fdtd_b200_set_progress": (i32, [vp, i32, i32, i32]),
     "fdtd_b200_launch_count": (C.c_longlong, [vp]),
     "fdtd_b200_last_error": (C.c_char_p, []),
 }

@@ -1408,26 +1408,30 @@ int fdtd_b200_device_fields(const AcousticFDTDState* st, void** out5)
     return FDTD_OK;
 }
 
-// The step counter and the stability check's rotating phase: with the
-// current P and V fields they are the whole state a later step depends on
-// (the source schedule and receivers are configuration), so a snapshot of
-// the five fields plus these two resumes a room exactly.
-int fdtd_b200_get_progress(const AcousticFDTDState* st, int* step_count, int* check_phase)
+// The step counter, the stability check's rotating phase and the step whose
+// source sample is already in P (a batch deposits the next step's sample
+// ahead): with the current P and V fields they are the whole state a later
+// step depends on (the source schedule and receivers are configuration), so
+// a snapshot of the fields plus these three resumes a room exactly.
+int fdtd_b200_get_progress(const AcousticFDTDState* st, int* step_count, int* check_phase, int* deposited_step)
 {
-    if (!st || !step_count || !check_phase) return FDTD_ERR_NULL;
+    if (!st || !step_count || !check_phase || !deposited_step) return FDTD_ERR_NULL;
     *step_count = st->step_count;
     *check_phase = st->stab_phase;
+    *deposited_step = st->ps_done_step;
     return FDTD_OK;
 }
 
-int fdtd_b200_set_progress(AcousticFDTDState* st, int step_count, int check_phase)
+int fdtd_b200_set_progress(AcousticFDTDState* st, int step_count, int check_phase, int deposited_step)
 {
     if (!st) return FDTD_ERR_NULL;
-    if (step_count < 0 || check_phase < 0 || check_phase >= kCheckStride) return FDTD_ERR_ARG;
+    if (step_count < 0 || check_phase < 0 || check_phase >= kCheckStride || deposited_step < -1)
+        return FDTD_ERR_ARG;
     if (dev_guard(st)) return FDTD_ERR_CUDA;
     CK(cudaStreamSynchronize(st->stream));
     st->step_count = step_count;
     st->stab_phase = check_phase;
+    st->ps_done_step = deposited_step;
     return FDTD_OK;
 }
 

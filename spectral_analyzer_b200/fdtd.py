@@ -417,17 +417,18 @@ class AcousticFDTD:
 
     def snapshot(self) -> dict:
         """The room's state in host memory: the current P and V fields (the
-        device layout, padding included), the step count and the stability
-        check's phase.  ``restore`` on a handle of the same room configuration
+        device layout, padding included), the step count, the stability
+        check's phase and the step whose source sample P already holds.  ``restore`` on a handle of the same room configuration
         (source schedule, receivers) continues exactly as this one would."""
         import torch
         self.synchronize()
         f = self._device_fields()
-        step, phase = C.c_int(), C.c_int()
-        self._check(self._lib.fdtd_b200_get_progress(self._h, C.byref(step), C.byref(phase)), "get_progress")
+        step, phase, dep = C.c_int(), C.c_int(), C.c_int()
+        self._check(self._lib.fdtd_b200_get_progress(self._h, C.byref(step), C.byref(phase), C.byref(dep)),
+                    "get_progress")
         fields = [self._view(f[q]).to("cpu") for q in (0, 2, 3, 4)]
         torch.cuda.synchronize(self.device)
-        return {"step": step.value, "phase": phase.value, "fields": fields,
+        return {"step": step.value, "phase": phase.value, "deposited": dep.value, "fields": fields,
                 "dims": (self.Nx, self.Ny, self.Nz)}
 
     def restore(self, snap: dict):
@@ -440,8 +441,8 @@ class AcousticFDTD:
             self._view(f[q]).copy_(t)
         import torch
         torch.cuda.synchronize(self.device)
-        self._check(self._lib.fdtd_b200_set_progress(self._h, int(snap["step"]), int(snap["phase"])),
-                    "set_progress")
+        self._check(self._lib.fdtd_b200_set_progress(self._h, int(snap["step"]), int(snap["phase"]),
+                                                     int(snap["deposited"])), "set_progress")
 
     def profile(self, enable: bool = True):
         self._check(self._lib.fdtd_b200_profile(self._h, 1 if enable else 0), "profile")
