@@ -183,6 +183,18 @@ __device__ __forceinline__ float4 vel4(const Coef& cf, const float4& pm, const f
     return r;
 }
 
+// four faces, 2nd-order gradient, given damping (the faces next to a j end)
+__device__ __forceinline__ float4 vel4_2nd(const Coef& cf, const float4& p0, const float4& p1,
+                                          const float4& vo, const float4& dmp)
+{
+    float4 r;
+    r.x = vupd(cf, vo.x, fsub(p1.x, p0.x), dmp.x);
+    r.y = vupd(cf, vo.y, fsub(p1.y, p0.y), dmp.y);
+    r.z = vupd(cf, vo.z, fsub(p1.z, p0.z), dmp.z);
+    r.w = vupd(cf, vo.w, fsub(p1.w, p0.w), dmp.w);
+    return r;
+}
+
 // as vel4, with a per-face gradient order (bit q of m4) and existence (bit q of ok)
 __device__ __forceinline__ float4 vel4_masked(const Coef& cf, float4 pm, float4 p0, float4 p1,
                                              float4 p2, float4 vo, float4 dmp, int m4, int ok)
@@ -401,15 +413,17 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
     float axw3 = ax_at(u0 - 3), axw2 = ax_at(u0 - 2), axw1 = ax_at(u0 - 1), axw0 = ax_at(u0);
     float pxw = px_at(u0 - 3);
 
-    // The interior iterations of a clean tile take a separately compiled body
-    // without the general path (a general path present in the loop costs the
-    // interior about 12 % although it never runs there).  Iteration u is
-    // interior when plane u-3 and faces u-2 .. u-1 have no x absorption, face
-    // u-2 has the 4th-order gradient and the planes u-3, u-2 are own ones; a
-    // tile is clean when every row of its Vy faces has the 4th-order gradient
-    // and all its columns are cells.  Both bodies evaluate the same expressions
-    // (alpha_x = 0, px = 1 there), so the results do not depend on the choice.
-    const bool clean = kfull && j0 - 2 >= 1 && j0 + C::TJ <= ny - 3;
+    // The interior iterations of a tile whose columns are all cells take a
+    // separately compiled body without the general path (the general path
+    // present in the loop costs the interior about 12 % although it never runs
+    // there).  Iteration u is interior when plane u-3 and faces u-2 .. u-1 have
+    // no x absorption, face u-2 has the 4th-order gradient and the planes u-3,
+    // u-2 are own ones.  Rows beyond the room and Vy faces at the j ends are
+    // warp-uniform cases the interior body handles itself.  Both bodies
+    // evaluate the same expressions (alpha_x = 0, px = 1 there), so the results
+    // do not depend on the choice.  The step runs in one wave, so a CTA left on
+    // the general body for its whole march would set the kernel's time.
+    const bool clean = kfull;
     int fast_lo = u1 + 1, fast_hi = u1 + 1;
     if (clean && a.tb.xi_hi > a.tb.xi_lo) {
         fast_lo = max(max(a.tb.xi_lo + 3, 3 - xg0), i_beg + 3);
@@ -458,7 +472,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
         if (FAST || u >= i_beg) {
             const int f = u - 2, fg = f + xg0;
             float4 vnew = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (FAST || (fg >= 0 && fg <= nxg - 2 && row_ok)) {
+            if (FAST ? row_ok : (fg >= 0 && fg <= nxg - 2 && row_ok)) {
                 const float4 pm = lds4(smem + C::RING0 + pslot[0] * C::P_STAGE + cP);
                 const float4 p0 = lds4(smem + C::RING0 + pslot[1] * C::P_STAGE + cP);
                 const float4 p1 = lds4(smem + C::RING0 + pslot[2] * C::P_STAGE + cP);
@@ -483,7 +497,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                         vnew = vel4_general(cf, pm, p0, p1, p2, vo, aL, aR, fourth ? 15 : 0, okx);
                     }
                 }
-                if (f >= i_beg && f < i_end && (FAST || st_ok)) {
+                if (f >= i_beg && f < i_end && st_ok) {
                     stg4(a.vout[0] + f * PL + own, vnew);
 #pragma unroll
                     for (int sd = 0; sd < 2; ++sd)   // the neighbours' ghost faces
@@ -512,13 +526,15 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                     if (r < C::VYR) {
                         const int jf = j0 - 2 + r;
                         float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                        if (FAST || (jf >= 0 && jf <= ny - 2)) {
+                        if (jf >= 0 && jf <= ny - 2) {
                             const float* pc = pst + 4 * lane + 4;
                             const float4 pm = lds4(pc + r * C::PC), p0 = lds4(pc + (r + 1) * C::PC);
                             const float4 p1 = lds4(pc + (r + 2) * C::PC), p2 = lds4(pc + (r + 3) * C::PC);
                             const float4 vo = lds4(vys + r * C::TK + 4 * lane);
                             if constexpr (FAST) {
-                                v = vel4(cf, pm, p0, p1, p2, vo, dyi[m]);
+                                // the row's gradient order is uniform over its threads
+                                if (jf > 0 && jf < ny - 2) v = vel4(cf, pm, p0, p1, p2, vo, dyi[m]);
+                                else v = vel4_2nd(cf, p0, p1, vo, dyi[m]);
                             } else {
                                 const bool fourth = (jf > 0 && jf < ny - 2);
                                 if (fourth && xint && kfull) {
@@ -548,7 +564,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                 {
                     const float* prow = pst + (w + 3) * C::PC;
                     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (FAST || row_ok) {
+                    if (row_ok) {
                         const int c = 4 * lane + 4;            // col of kb
                         pown = lds4(prow + c);
                         const float4 pb4 = lds4(prow + c + 4);
@@ -570,7 +586,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                             }
                             v = vel4_general(cf, pm, pown, p1, p2, vo, aL, aR, zm4, zok);
                         }
-                        if (FAST || st_ok) stg4(a.vout[2] + ib + own, v);
+                        if (st_ok) stg4(a.vout[2] + ib + own, v);
                     }
                     sts4(vzn + w * C::PC + 4 * lane + 4, v);
                 }
@@ -583,7 +599,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                     const int kf = k0 - 4 + ch;
                     const float* prow = pst + (jl + 3) * C::PC;
                     float vh = 0.0f;
-                    if ((FAST || j0 + jl < ny) && kf >= 0 && kf <= nz - 2) {
+                    if (j0 + jl < ny && kf >= 0 && kf <= nz - 2) {
                         const bool fourth = (kf > 0 && kf < nz - 2);
                         const float ay = ay_s[jl + 2];
                         const float gr = grad4(cf, prow[ch - 1], prow[ch], prow[ch + 1], prow[ch + 2], fourth);
@@ -596,7 +612,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                 __syncthreads();
 
                 // P^{n+1} of the own cells
-                if (FAST || row_ok) {
+                if (row_ok) {
                     const float* yr = vyn + 4 * lane;
                     const float4 ymm = lds4(yr + w * C::TK), ym = lds4(yr + (w + 1) * C::TK);
                     const float4 yp = lds4(yr + (w + 2) * C::TK), ypp = lds4(yr + (w + 3) * C::TK);
@@ -621,7 +637,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                         for (int q = 0; q < 4; ++q)
                             if (kb + q >= nz) at(out, q) = 0.0f;
                     }
-                    if (FAST || kb < sz) {
+                    if (kb < sz) {
                         stg4(a.pn + ib + own, out);
 #pragma unroll
                         for (int sd = 0; sd < 2; ++sd)   // the neighbours' ghost planes
