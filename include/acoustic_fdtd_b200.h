@@ -326,7 +326,11 @@ FDTD_B200_API long long fdtd_b200_batch_launch_count(const FdtdB200Batch* b);
  * FP16 fields are stored times p_scale (P) or v_scale (V), powers of two
  * (<= 0 picks 2^10 and 2^19, right for source samples of order 1).
  * Sources are deposited before a step, receivers (8 taps, summed in double)
- * record after it, as fdtd_step + fdtd_sample_pressure_precomputed do. */
+ * record after it, as fdtd_step + fdtd_sample_pressure_precomputed do.
+ * The 16-bit modes (2-5) step by default with a single-pass kernel that
+ * reads and writes each stored field once (fdtd_b200_prec_set_kernel); it
+ * produces the two-pass update's stored bits, and steps that take an energy
+ * audit run the two-pass update. */
 typedef struct FdtdB200Prec FdtdB200Prec;
 FDTD_B200_API FdtdB200Prec* fdtd_b200_prec_create(int Nx, int Ny, int Nz, double dx, double c,
                                                   double rho_air, int n_pml, const float* a6,
@@ -353,6 +357,14 @@ FDTD_B200_API int fdtd_b200_prec_get_energy(FdtdB200Prec* p, double* out3, int o
                                             int* n_out);
 /* Current pressure, reference cell order, widened to double. */
 FDTD_B200_API int fdtd_b200_prec_get_pressure(FdtdB200Prec* p, double* out, int out_len);
+/* Step kernel of a 16-bit mode: 1 single pass (the default), 0 two-pass.
+ * FDTD_ERR_ARG for 1 in the FP32 / FP64 modes. */
+FDTD_B200_API int fdtd_b200_prec_set_kernel(FdtdB200Prec* p, int kernel);
+FDTD_B200_API int fdtd_b200_prec_get_kernel(const FdtdB200Prec* p);
+/* Kernels launched by fdtd_b200_prec_step since create. */
+FDTD_B200_API long long fdtd_b200_prec_launch_count(const FdtdB200Prec* p);
+/* The handle's CUDA stream (cudaStream_t), for events around its steps. */
+FDTD_B200_API void* fdtd_b200_prec_stream(const FdtdB200Prec* p);
 
 /* ---- gradient w.r.t. per-cell absorption (no reference counterpart) ----
  * An open room whose absorption is a per-cell field a_c = alpha_c * dt in

@@ -89,6 +89,10 @@ SIGNATURES = {
     "fdtd_b200_prec_get_traces": (i32, [vp, P_f64, i32, P_i32]),
     "fdtd_b200_prec_get_energy": (i32, [vp, P_f64, i32, P_i32]),
     "fdtd_b200_prec_get_pressure": (i32, [vp, P_f64, i32]),
+    "fdtd_b200_prec_set_kernel": (i32, [vp, i32]),
+    "fdtd_b200_prec_get_kernel": (i32, [vp]),
+    "fdtd_b200_prec_launch_count": (C.c_longlong, [vp]),
+    "fdtd_b200_prec_stream": (vp, [vp]),
     "fdtd_b200_adj_create": (vp, [i32, i32, i32, C.c_double, C.c_double, C.c_double, i32, i32, i32]),
     "fdtd_b200_adj_destroy": (None, [vp]),
     "fdtd_b200_adj_dt": (C.c_double, [vp]),

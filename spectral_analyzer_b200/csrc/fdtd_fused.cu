@@ -38,6 +38,7 @@
  * and to the reference.
  */
 #include "fdtd_internal.h"
+#include "fdtd_tma.h"
 
 #include <cuda.h>
 #include <cudaTypedefs.h>
@@ -97,61 +98,6 @@ struct Cfg {
     static_assert(LW == 32 || LW == 16, "a row is one warp or half a warp");
     static_assert(TJ % RW == 0 && HW * 32 <= NT, "whole warps of rows; halo warps exist");
 };
-
-__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(unsigned bar, unsigned count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(unsigned bar, unsigned bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(unsigned bar, unsigned parity)
-{
-    unsigned ok;
-    asm volatile(
-        "{\n .reg .pred p;\n"
-        " mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
-    return ok != 0;
-}
-
-__device__ __forceinline__ unsigned long long global_ns()
-{
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
-    return t;
-}
-
-// Bounded wait for the phase with the given parity: polls until it completes,
-// limit_us of wall time has passed, or kWaitPolls polls were made (whichever
-// comes first); false when a bound ran out.  The first 8 polls read no clock
-// (most waits end within them, and the clock read costs the march 1 %).
-__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity, unsigned limit_us)
-{
-    for (int it = 0; it < 8; ++it)
-        if (mbar_try(bar, parity)) return true;
-    const unsigned long long t0 = global_ns(), limit = 1000ull * limit_us;
-    for (int it = 0; it < kWaitPolls; ++it) {
-        if (mbar_try(bar, parity)) return true;
-        if (global_ns() - t0 > limit) return false;
-    }
-    return false;
-}
-
-__device__ __forceinline__ void tma_load3(unsigned dst, const CUtensorMap* map, int x, int y, int z,
-                                          unsigned bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4}], [%5];\n"
-        ::"r"(dst), "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar) : "memory");
-}
 
 __device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
 __device__ __forceinline__ void sts4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
@@ -270,13 +216,6 @@ __device__ __forceinline__ void init_barriers(unsigned bar0)
 
 // One tile (TJ x TK columns, planes [seg*seg_len, ...)) of the fused step.
 // Returns false when a load wait ran out (the CTA must stop; status is set).
-// Make the tensor map at `map` (in global memory, rewritten by a host copy since
-// it was last used) visible to the TMA unit instead of a cached older copy.
-__device__ __forceinline__ void acquire_tensormap(const CUtensorMap* map)
-{
-    asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;\n" ::"l"(map) : "memory");
-}
-
 // PEER = false compiles out the neighbour ghost-plane stores (single rooms and
 // batches), which the slab step of a split room needs.
 template <class C, bool PEER = true>
@@ -824,6 +763,9 @@ int g_slots_per_sm[2][kMaxDevices];   // per tile shape and device
 int g_sms[2][kMaxDevices];
 bool g_configured[2][kMaxDevices];
 
+}  // namespace
+
+namespace {
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
 std::once_flag g_encode_once;
 
@@ -838,23 +780,24 @@ cudaError_t get_encoder()
     });
     return g_encode ? cudaSuccess : cudaErrorNotSupported;
 }
+}  // namespace
 
-// A 3-D map over one padded field [nx][ny][sz] with a (bx, by, 1) box.
-cudaError_t encode_map(CUtensorMap* m, const float* base, const Grid& g, int bx, int by)
+cudaError_t encode_field_map(CUtensorMap* m, const void* base, int elem_bytes, const Grid& g, int bx, int by)
 {
     cudaError_t e = get_encoder();
     if (e != cudaSuccess) return e;
+    if (elem_bytes != 4 && elem_bytes != 2) return cudaErrorInvalidValue;
+    const cuuint64_t eb = (cuuint64_t)elem_bytes;
     cuuint64_t dims[3] = {(cuuint64_t)g.sz, (cuuint64_t)g.ny, (cuuint64_t)g.nx};
-    cuuint64_t strides[2] = {(cuuint64_t)g.sz * 4, (cuuint64_t)g.plane * 4};
+    cuuint64_t strides[2] = {(cuuint64_t)g.sz * eb, (cuuint64_t)g.plane * eb};
     cuuint32_t box[3] = {(cuuint32_t)bx, (cuuint32_t)by, 1};
     cuuint32_t es[3] = {1, 1, 1};
-    CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<float*>(base), dims, strides,
-                          box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    CUresult r = g_encode(m, elem_bytes == 4 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_UINT16, 3,
+                          const_cast<void*>(base), dims, strides, box, es, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     return r == CUDA_SUCCESS ? cudaSuccess : cudaErrorInvalidValue;
 }
-
-}  // namespace
 
 struct FusedCache {
     struct Entry {
@@ -889,7 +832,7 @@ static cudaError_t cached_map(FusedCache* c, const float* base, int kind, const 
     e.base = base;
     e.kind = kind;
     e.shape = shape;
-    cudaError_t err = encode_map(&e.map, base, g, bx, by);
+    cudaError_t err = encode_field_map(&e.map, base, 4, g, bx, by);
     if (err != cudaSuccess) return err;
     c->entries.push_back(e);
     *out = e.map;

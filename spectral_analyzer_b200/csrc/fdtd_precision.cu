@@ -30,6 +30,7 @@
  */
 #include "acoustic_fdtd_b200.h"
 #include "fdtd_internal.h"
+#include "fdtd_prec_internal.h"
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -42,89 +43,6 @@
 
 namespace fdtd {
 namespace prec {
-
-enum Mode { kFP32 = 0, kFP64 = 1, kBF16 = 2, kFP16 = 3, kBF16C = 4, kFP16C = 5 };
-
-// exactly rounded ops in both arithmetic types
-__device__ __forceinline__ float radd(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float rsub(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float rmul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ double radd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double rsub(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ double rmul(double a, double b) { return __dmul_rn(a, b); }
-
-template <int M> struct Traits;
-template <> struct Traits<kFP32> { using A = float; using S = float; static constexpr bool comp = false; };
-template <> struct Traits<kFP64> { using A = double; using S = double; static constexpr bool comp = false; };
-template <> struct Traits<kBF16> { using A = float; using S = __nv_bfloat16; static constexpr bool comp = false; };
-template <> struct Traits<kFP16> { using A = float; using S = __half; static constexpr bool comp = false; };
-template <> struct Traits<kBF16C> { using A = float; using S = __nv_bfloat16; static constexpr bool comp = true; };
-template <> struct Traits<kFP16C> { using A = float; using S = __half; static constexpr bool comp = true; };
-
-__device__ __forceinline__ float tofl(float v) { return v; }
-__device__ __forceinline__ double tofl(double v) { return v; }
-__device__ __forceinline__ float tofl(__nv_bfloat16 v) { return __bfloat162float(v); }
-__device__ __forceinline__ float tofl(__half v) { return __half2float(v); }
-template <class S> __device__ __forceinline__ S fromfl(float v);
-template <> __device__ __forceinline__ float fromfl<float>(float v) { return v; }
-template <> __device__ __forceinline__ __nv_bfloat16 fromfl<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
-template <> __device__ __forceinline__ __half fromfl<__half>(float v) { return __float2half_rn(v); }
-
-// One stored field: value array, optional residual array, power-of-two scale.
-struct Field {
-    void* hi;
-    void* lo;
-    float scale, inv_scale;        // stored value = x * scale
-    float lo_scale, inv_lo_scale;  // stored residual = (x*scale - hi) * lo_scale
-};
-
-template <int M>
-__device__ __forceinline__ typename Traits<M>::A ld(const Field& f, long long i)
-{
-    using T = Traits<M>;
-    using S = typename T::S;
-    if constexpr (M == kFP32 || M == kFP64) {
-        return static_cast<const S*>(f.hi)[i];
-    } else {
-        float v = tofl(static_cast<const S*>(f.hi)[i]);
-        if constexpr (T::comp)
-            v = __fadd_rn(v, __fmul_rn(tofl(static_cast<const S*>(f.lo)[i]), f.inv_lo_scale));
-        return __fmul_rn(v, f.inv_scale);
-    }
-}
-
-template <int M>
-__device__ __forceinline__ void st(const Field& f, long long i, typename Traits<M>::A x)
-{
-    using T = Traits<M>;
-    using S = typename T::S;
-    if constexpr (M == kFP32 || M == kFP64) {
-        static_cast<S*>(f.hi)[i] = x;
-    } else {
-        const float xs = __fmul_rn(x, f.scale);
-        const S h = fromfl<S>(xs);
-        static_cast<S*>(f.hi)[i] = h;
-        if constexpr (T::comp)
-            static_cast<S*>(f.lo)[i] = fromfl<S>(__fmul_rn(__fsub_rn(xs, tofl(h)), f.lo_scale));
-    }
-}
-
-template <class A>
-struct PCoef {
-    A vc, bulk, dt, c1, c2;
-    const A *ax, *ay, *az, *px, *py, *pz;
-};
-
-template <class A>
-__device__ __forceinline__ A fdamp(A aL, A aR, A dt)
-{
-    return rsub(A(1), rmul(rmul(A(0.5), radd(aL, aR)), dt));
-}
-
-template <class A>
-__device__ __forceinline__ A amax(A a, A b) { return a > b ? a : b; }
-template <class A>
-__device__ __forceinline__ A amin(A a, A b) { return a < b ? a : b; }
 
 __device__ __forceinline__ double block_sum(double v)
 {
@@ -140,57 +58,6 @@ __device__ __forceinline__ double block_sum(double v)
         for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
     }
     return s;   // valid in thread (0,0)
-}
-
-// Four consecutive values (index i a multiple of 4, so the access is aligned:
-// rows start on 8-element boundaries).  Each value is decoded exactly as ld().
-template <int M>
-__device__ __forceinline__ void ld4(const Field& f, long long i, typename Traits<M>::A (&v)[4])
-{
-    using T = Traits<M>;
-    using S = typename T::S;
-    if constexpr (M == kFP32) {
-        const float4 x = *reinterpret_cast<const float4*>(static_cast<const float*>(f.hi) + i);
-        v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w;
-    } else if constexpr (M == kFP64) {
-        const double2 x = *reinterpret_cast<const double2*>(static_cast<const double*>(f.hi) + i);
-        const double2 y = *reinterpret_cast<const double2*>(static_cast<const double*>(f.hi) + i + 2);
-        v[0] = x.x; v[1] = x.y; v[2] = y.x; v[3] = y.y;
-    } else {
-        union { uint2 u; S s[4]; } h, l;
-        h.u = *reinterpret_cast<const uint2*>(static_cast<const S*>(f.hi) + i);
-        if constexpr (T::comp) l.u = *reinterpret_cast<const uint2*>(static_cast<const S*>(f.lo) + i);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            float x = tofl(h.s[q]);
-            if constexpr (T::comp) x = __fadd_rn(x, __fmul_rn(tofl(l.s[q]), f.inv_lo_scale));
-            v[q] = __fmul_rn(x, f.inv_scale);
-        }
-    }
-}
-
-// Four consecutive values, each encoded exactly as st().
-template <int M>
-__device__ __forceinline__ void st4(const Field& f, long long i, const typename Traits<M>::A (&v)[4])
-{
-    using T = Traits<M>;
-    using S = typename T::S;
-    if constexpr (M == kFP32) {
-        *reinterpret_cast<float4*>(static_cast<float*>(f.hi) + i) = make_float4(v[0], v[1], v[2], v[3]);
-    } else if constexpr (M == kFP64) {
-        *reinterpret_cast<double2*>(static_cast<double*>(f.hi) + i) = make_double2(v[0], v[1]);
-        *reinterpret_cast<double2*>(static_cast<double*>(f.hi) + i + 2) = make_double2(v[2], v[3]);
-    } else {
-        union { uint2 u; S s[4]; } h, l;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const float xs = __fmul_rn(v[q], f.scale);
-            h.s[q] = fromfl<S>(xs);
-            if constexpr (T::comp) l.s[q] = fromfl<S>(__fmul_rn(__fsub_rn(xs, tofl(h.s[q])), f.lo_scale));
-        }
-        *reinterpret_cast<uint2*>(static_cast<S*>(f.hi) + i) = h.u;
-        if constexpr (T::comp) *reinterpret_cast<uint2*>(static_cast<S*>(f.lo) + i) = l.u;
-    }
 }
 
 #define PREC_INDEX                                                        \
@@ -389,6 +256,16 @@ struct FdtdB200Prec {
     void* d_tab = nullptr;
     Field f[5] = {};            // P0, P1, Vx, Vy, Vz
     int cur = 0;                // P current = f[cur]
+    // The single-pass 16-bit step writes the other velocity set (v2) and
+    // flips vset; the two-pass step updates the current set in place.
+    int kernel = 0;             // 1: single-pass step (16-bit modes), 0: two-pass
+    Field v2[3] = {};
+    int vset = 0;
+    F16Cache* maps = nullptr;
+    unsigned* d_status = nullptr;
+    std::vector<double> h_sig; // host copy of the source signal (the launch argument)
+    bool rec_pending = false;   // the current P's receivers are not recorded yet
+    long long launches = 0;     // kernels launched by prec_step
     std::vector<void*> allocs;
     long long src = -1;
     double* d_sig = nullptr;
@@ -405,6 +282,8 @@ struct FdtdB200Prec {
 };
 
 namespace {
+
+Field* vfields(FdtdB200Prec* p) { return p->vset ? p->v2 : p->f + 2; }
 
 size_t elem_bytes(int mode) { return mode == kFP64 ? 8 : mode == kFP32 ? 4 : 2; }
 bool compensated(int mode) { return mode == kBF16C || mode == kFP16C; }
@@ -473,6 +352,89 @@ int fail(cudaError_t e, const char* what)
 #define PCK(x) do { cudaError_t e_ = (x); if (e_ != cudaSuccess) return fail(e_, #x); } while (0)
 
 template <int M>
+void record_now(FdtdB200Prec* p)
+{
+    if (p->n_rec > 0 && p->n_rec_steps < p->cap) {
+        k_src_rec<M><<<1, 128, 0, p->stream>>>(p->f[p->cur], -1, nullptr, 0, 0, p->n_rec, p->d_ridx, p->d_rw,
+                                               p->d_trace + (size_t)p->n_rec_steps * p->n_rec, 1);
+        ++p->n_rec_steps;
+        ++p->launches;
+    }
+}
+
+// the second velocity set of the single-pass step, zeroed (faces it never
+// writes — the last face of each axis and the row padding — stay zero)
+int ensure_v2(FdtdB200Prec* p)
+{
+    if (p->v2[0].hi) return FDTD_OK;
+    const size_t fb = (size_t)p->g.cells * elem_bytes(p->mode);
+    for (int q = 0; q < 3; ++q) {
+        Field& f = p->v2[q];
+        f = p->f[2 + q];
+        f.hi = f.lo = nullptr;
+        PCK(cudaMalloc(&f.hi, fb));
+        p->allocs.push_back(f.hi);
+        PCK(cudaMemset(f.hi, 0, fb));
+        if (compensated(p->mode)) {
+            PCK(cudaMalloc(&f.lo, fb));
+            p->allocs.push_back(f.lo);
+            PCK(cudaMemset(f.lo, 0, fb));
+        }
+    }
+    return FDTD_OK;
+}
+
+// one single-pass step (16-bit modes): P^n, V set -> P^{n+1}, other V set;
+// records the previous step's receivers from P^n when they are pending
+template <int M>
+int fused16_step(FdtdB200Prec* p)
+{
+    const int rc = ensure_v2(p);
+    if (rc != FDTD_OK) return rc;
+    const Grid& g = p->g;
+    Field* vin = vfields(p);
+    Field* vout = p->vset ? p->f + 2 : p->v2;
+    const Field& P = p->f[p->cur];
+    const Field& PN = p->f[p->cur ^ 1];
+    F16Args a{};
+    a.g = g;
+    a.cf = p->cf32;
+    a.p_hi = P.hi; a.p_lo = P.lo;
+    a.pn_hi = PN.hi; a.pn_lo = PN.lo;
+    for (int q = 0; q < 3; ++q) {
+        a.vout_hi[q] = vout[q].hi;
+        a.vout_lo[q] = vout[q].lo;
+    }
+    a.sp = Sc{P.scale, P.inv_scale, P.lo_scale, P.inv_lo_scale};
+    a.sv = Sc{vin[0].scale, vin[0].inv_scale, vin[0].lo_scale, vin[0].inv_lo_scale};
+    a.dep_amp = 0.0f;
+    a.dep_i = -1000;
+    if (p->src >= 0 && p->step < p->n_sig) {
+        a.dep_amp = (float)p->h_sig[p->step];
+        a.dep_i = (int)(p->src / g.plane);
+        a.dep_j = (int)((p->src % g.plane) / g.sz);
+        a.dep_k = (int)(p->src % g.sz);
+    }
+    if (p->rec_pending && p->n_rec > 0 && p->n_rec_steps < p->cap) {
+        a.n_rec = p->n_rec;
+        a.rec_idx = p->d_ridx;
+        a.rec_w = p->d_rw;
+        a.rec_out = p->d_trace + (size_t)p->n_rec_steps * p->n_rec;
+        ++p->n_rec_steps;
+    }
+    a.status = p->d_status;
+    a.wait_us = kWaitUs;
+    const void* bases[8] = {P.hi, P.lo, vin[0].hi, vin[0].lo, vin[1].hi, vin[1].lo, vin[2].hi, vin[2].lo};
+    PCK(launch_fused16(p->mode, a, p->maps, bases, p->stream));
+    ++p->launches;
+    p->cur ^= 1;
+    p->vset ^= 1;
+    ++p->step;
+    p->rec_pending = true;
+    return FDTD_OK;
+}
+
+template <int M>
 int step_impl(FdtdB200Prec* p, int n, int audit_every)
 {
     using A = typename Traits<M>::A;
@@ -480,28 +442,54 @@ int step_impl(FdtdB200Prec* p, int n, int audit_every)
     const Grid& g = p->g;
     dim3 block(32, 8, 1), grid((g.sz / 4 + 31) / 32, (g.ny + 7) / 8, g.nx);
     for (int s = 0; s < n; ++s) {
+        const bool audit = audit_every > 0 && p->step % audit_every == 0;
+        if constexpr (M == kBF16 || M == kFP16 || M == kBF16C || M == kFP16C) {
+            if (p->kernel == 1 && !audit) {
+                const int rc = fused16_step<M>(p);
+                if (rc != FDTD_OK) return rc;
+                continue;
+            }
+        }
+        if (p->rec_pending) {
+            record_now<M>(p);
+            p->rec_pending = false;
+        }
         Field& P = p->f[p->cur];
         Field& PN = p->f[p->cur ^ 1];
+        Field* V = vfields(p);
         k_src_rec<M><<<1, 32, 0, p->stream>>>(P, p->src, p->d_sig, p->step, p->n_sig, 0, nullptr, nullptr,
                                               nullptr, 0);
         double* aud = nullptr;
-        if (audit_every > 0 && p->step % audit_every == 0) {
+        if (audit) {
             if ((int)p->audit_steps.size() >= p->cap_audit) return FDTD_ERR_DIM;
             aud = p->d_audit + 2 * p->audit_steps.size();
             PCK(cudaMemsetAsync(aud, 0, 2 * sizeof(double), p->stream));
             p->audit_steps.push_back(p->step);
         }
-        k_vel<M><<<grid, block, 0, p->stream>>>(g, cf, P, p->f[2], p->f[3], p->f[4], aud);
-        k_pres<M><<<grid, block, 0, p->stream>>>(g, cf, P, PN, p->f[2], p->f[3], p->f[4]);
+        k_vel<M><<<grid, block, 0, p->stream>>>(g, cf, P, V[0], V[1], V[2], aud);
+        k_pres<M><<<grid, block, 0, p->stream>>>(g, cf, P, PN, V[0], V[1], V[2]);
+        p->launches += 3;
         p->cur ^= 1;
         ++p->step;
-        if (p->n_rec > 0 && p->n_rec_steps < p->cap) {
-            k_src_rec<M><<<1, 128, 0, p->stream>>>(p->f[p->cur], -1, nullptr, 0, 0, p->n_rec, p->d_ridx,
-                                                   p->d_rw, p->d_trace + (size_t)p->n_rec_steps * p->n_rec, 1);
-            ++p->n_rec_steps;
-        }
+        record_now<M>(p);
+    }
+    if (p->rec_pending) {
+        record_now<M>(p);
+        p->rec_pending = false;
     }
     PCK(cudaGetLastError());
+    return FDTD_OK;
+}
+
+// a load wait of the single-pass step that ran out (status word set)
+int check_status(FdtdB200Prec* p)
+{
+    unsigned st[kStatusWords];
+    PCK(cudaMemcpy(st, p->d_status, sizeof(st), cudaMemcpyDeviceToHost));
+    if (st[kStatusTimeout] != 0xFFFFFFFFu) {
+        record_cuda_error(cudaErrorLaunchTimeout, "fdtd_b200_prec_step: load wait timed out");
+        return FDTD_ERR_CUDA;
+    }
     return FDTD_OK;
 }
 
@@ -560,10 +548,14 @@ FdtdB200Prec* fdtd_b200_prec_create(int Nx, int Ny, int Nz, double dx, double c,
             if (ok) p->allocs.push_back(f.lo);
         }
     }
+    ok = ok && cudaMalloc(&p->d_status, sizeof(unsigned) * kStatusWords) == cudaSuccess &&
+         cudaMemset(p->d_status, 0xFF, sizeof(unsigned) * kStatusWords) == cudaSuccess;
     if (!ok) {
         fdtd_b200_prec_destroy(p);
         return nullptr;
     }
+    p->maps = f16_cache_create();
+    p->kernel = f16_supported(mode, p->g) ? 1 : 0;
     return p;
 }
 
@@ -579,6 +571,8 @@ void fdtd_b200_prec_destroy(FdtdB200Prec* p)
     cudaFree(p->d_rw);
     cudaFree(p->d_trace);
     cudaFree(p->d_audit);
+    cudaFree(p->d_status);
+    f16_cache_destroy(p->maps);
     if (p->stream) cudaStreamDestroy(p->stream);
     delete p;
 }
@@ -593,12 +587,14 @@ int fdtd_b200_prec_set_source(FdtdB200Prec* p, int cell, const double* signal, i
     cudaFree(p->d_sig);
     p->d_sig = nullptr;
     p->n_sig = 0;
+    p->h_sig.clear();
     const int nz = p->g.nz, ny = p->g.ny;
     p->src = ((long long)(cell / nz / ny) * ny + (cell / nz) % ny) * p->g.sz + cell % nz;
     if (n > 0) {
         PCK(cudaMalloc(&p->d_sig, sizeof(double) * n));
         PCK(cudaMemcpy(p->d_sig, signal, sizeof(double) * n, cudaMemcpyHostToDevice));
         p->n_sig = n;
+        p->h_sig.assign(signal, signal + n);
     }
     return FDTD_OK;
 }
@@ -648,12 +644,28 @@ int fdtd_b200_prec_step(FdtdB200Prec* p, int n_steps, int audit_every)
     }
 }
 
+int fdtd_b200_prec_set_kernel(FdtdB200Prec* p, int kernel)
+{
+    if (!p) return FDTD_ERR_NULL;
+    if (kernel != 0 && kernel != 1) return FDTD_ERR_ARG;
+    if (kernel == 1 && !f16_supported(p->mode, p->g)) return FDTD_ERR_ARG;
+    p->kernel = kernel;
+    return FDTD_OK;
+}
+
+int fdtd_b200_prec_get_kernel(const FdtdB200Prec* p) { return p ? p->kernel : -1; }
+
+long long fdtd_b200_prec_launch_count(const FdtdB200Prec* p) { return p ? p->launches : 0; }
+
+void* fdtd_b200_prec_stream(const FdtdB200Prec* p) { return p ? (void*)p->stream : nullptr; }
+
 int fdtd_b200_prec_get_traces(FdtdB200Prec* p, double* out, int out_len, int* n_recorded)
 {
     if (!p || !out) return FDTD_ERR_NULL;
     const long long need = (long long)p->n_rec_steps * p->n_rec;
     if (out_len < need) return FDTD_ERR_DIM;
     PCK(cudaStreamSynchronize(p->stream));
+    if (check_status(p) != FDTD_OK) return FDTD_ERR_CUDA;
     if (need > 0) PCK(cudaMemcpy(out, p->d_trace, sizeof(double) * need, cudaMemcpyDeviceToHost));
     if (n_recorded) *n_recorded = p->n_rec_steps;
     return FDTD_OK;
@@ -685,6 +697,7 @@ int fdtd_b200_prec_get_pressure(FdtdB200Prec* p, double* out, int out_len)
     if (!p || !out) return FDTD_ERR_NULL;
     if (out_len != p->N) return FDTD_ERR_DIM;
     PCK(cudaStreamSynchronize(p->stream));
+    if (check_status(p) != FDTD_OK) return FDTD_ERR_CUDA;
     const Field& f = p->f[p->cur];
     const size_t eb = elem_bytes(p->mode);
     std::vector<unsigned char> hi((size_t)p->g.cells * eb), lo;

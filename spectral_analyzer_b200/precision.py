@@ -81,7 +81,7 @@ class PrecisionRoom:
     """One room on the GPU with a chosen field storage."""
 
     def __init__(self, room: Room, mode: str, audit_capacity: int = 64, device: int = 0,
-                 trace_capacity: Optional[int] = None):
+                 trace_capacity: Optional[int] = None, kernel: str = "auto"):
         from . import _native
         if mode not in MODES:
             raise ValueError(f"unknown storage mode {mode!r}; one of {sorted(MODES)}")
@@ -110,6 +110,25 @@ class PrecisionRoom:
             self._h, self.n_rec, self._idx.ctypes.data_as(_native.P_i32),
             self._w.ctypes.data_as(_native.P_f64), int(cap), int(audit_capacity)), "prec_set_receivers")
         self.steps = 0
+        if kernel not in ("auto", "fused", "two_pass"):
+            raise ValueError(f"unknown kernel {kernel!r}; one of auto, fused, two_pass")
+        if kernel != "auto":
+            self._check(self._lib.fdtd_b200_prec_set_kernel(self._h, 1 if kernel == "fused" else 0),
+                        "prec_set_kernel")
+
+    @property
+    def kernel(self) -> str:
+        """The step kernel: "fused" (single pass, the 16-bit modes' default) or "two_pass"."""
+        return "fused" if self._lib.fdtd_b200_prec_get_kernel(self._h) == 1 else "two_pass"
+
+    def torch_stream(self):
+        """The handle's stream as a torch stream (CUDA events around steps)."""
+        import torch
+        return torch.cuda.ExternalStream(self._lib.fdtd_b200_prec_stream(self._h))
+
+    @property
+    def launch_count(self) -> int:
+        return int(self._lib.fdtd_b200_prec_launch_count(self._h))
 
     def _check(self, rc, what):
         if rc != 0:
@@ -158,11 +177,12 @@ class PrecisionRoom:
         return out.reshape(r.nx, r.ny, r.nz)
 
 
-def run_mode(room: Room, mode: str, audit_every: int = 500, chunk: int = 500, device: int = 0) -> dict:
+def run_mode(room: Room, mode: str, audit_every: int = 500, chunk: int = 500, device: int = 0,
+             kernel: str = "auto") -> dict:
     """Run the room in one storage mode; traces, energy log and wall time."""
     import torch
     cap = room.n_steps // audit_every + 2 if audit_every > 0 else 1
-    pr = PrecisionRoom(room, mode, audit_capacity=cap, device=device)
+    pr = PrecisionRoom(room, mode, audit_capacity=cap, device=device, kernel=kernel)
     torch.cuda.synchronize(device)
     t0 = time.perf_counter()
     left = room.n_steps

@@ -127,3 +127,66 @@ def test_invalid_arguments(cuda):
         assert lib.fdtd_b200_prec_step(h, 4, 1) == _native.FDTD_ERR_DIM   # audit log of size 0
     finally:
         lib.fdtd_b200_prec_destroy(h)
+
+
+SIXTEEN = ("bf16", "fp16", "bf16c", "fp16c")
+# room shapes: full and partial 128-column k tiles, rows beyond the last 8-row
+# tile, rooms thinner than the 4-plane stencil, more planes than one segment
+SHAPES = [(40, 36, 44), (37, 29, 23), (20, 24, 250), (33, 19, 129), (9, 5, 6), (150, 16, 128)]
+
+
+def _pair(room, mode):
+    from spectral_analyzer_b200.precision import PrecisionRoom
+    a = PrecisionRoom(room, mode, kernel="fused")
+    b = PrecisionRoom(room, mode, kernel="two_pass")
+    assert a.kernel == "fused" and b.kernel == "two_pass"
+    return a, b
+
+
+@pytest.mark.parametrize("mode", SIXTEEN)
+@pytest.mark.parametrize("dims", SHAPES)
+def test_single_pass_16bit_step_equals_two_pass(cuda, mode, dims):
+    """The single-pass 16-bit step stores the two-pass update's bits: pressure
+    field and receiver traces equal after steps taken in uneven calls."""
+    room = seeded_room(*dims, 90, seed=sum(dims), n_rec=3, n_pml=3, source_kind="ricker")
+    a, b = _pair(room, mode)
+    for n in (1, 40, 49):
+        a.step(n)
+    b.step(room.n_steps)
+    pa, pb = a.pressure(), b.pressure()
+    assert np.array_equal(pa.view(np.uint64), pb.view(np.uint64)), \
+        (mode, dims, int(np.sum(pa != pb)), float(np.max(np.abs(pa - pb))))
+    assert np.array_equal(a.traces().view(np.uint64), b.traces().view(np.uint64))
+    assert np.any(pa != 0.0)
+    # one launch per step, plus one receiver record at the end of each call
+    assert a.launch_count == room.n_steps + 3
+    a.close()
+    b.close()
+
+
+@pytest.mark.parametrize("mode", ("bf16c", "fp16"))
+def test_single_pass_mixes_with_audit_steps(cuda, mode):
+    """Steps that take the energy audit run the two-pass update on the current
+    velocity set; the result is unchanged and the energy log equals the
+    two-pass run's."""
+    from spectral_analyzer_b200.precision import PrecisionRoom
+    room = seeded_room(40, 36, 44, 120, seed=21, n_rec=3, n_pml=4, source_kind="ricker")
+    a = PrecisionRoom(room, mode, kernel="fused", audit_capacity=16)
+    b = PrecisionRoom(room, mode, kernel="two_pass", audit_capacity=16)
+    a.step(55, 25)
+    a.step(65, 25)
+    b.step(120, 25)
+    assert np.array_equal(a.pressure().view(np.uint64), b.pressure().view(np.uint64))
+    assert np.array_equal(a.traces().view(np.uint64), b.traces().view(np.uint64))
+    ea, eb = a.energy(), b.energy()
+    assert ea.shape == eb.shape and np.array_equal(ea[:, 0], eb[:, 0])
+    np.testing.assert_allclose(ea[:, 1:], eb[:, 1:], rtol=1e-12, atol=0)
+
+
+def test_single_pass_kernel_choice(cuda):
+    from spectral_analyzer_b200.precision import PrecisionRoom
+    room = seeded_room(16, 16, 16, 4, seed=3, n_rec=1, n_pml=2)
+    assert PrecisionRoom(room, "bf16").kernel == "fused"
+    assert PrecisionRoom(room, "fp32").kernel == "two_pass"
+    with pytest.raises(RuntimeError):
+        PrecisionRoom(room, "fp64", kernel="fused")
