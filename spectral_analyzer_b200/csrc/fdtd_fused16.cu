@@ -33,6 +33,7 @@
 #include "fdtd_tma.h"
 
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 namespace fdtd {
@@ -82,13 +83,16 @@ template <int M>
 struct Code {
     using S = typename Traits<M>::S;
     static constexpr bool C = Traits<M>::comp;
+    // the BF16 forms are stored unscaled (scale and residual scale 1), and a
+    // product with 1.0f is the operand itself, so those multiplies are left out
+    static constexpr bool U = (M == kBF16 || M == kBF16C);
     union U4 { uint2 u; S s[4]; };
 
     __device__ static float dec(S h, S l, const Sc& c)
     {
         float x = tofl(h);
-        if constexpr (C) x = __fadd_rn(x, __fmul_rn(tofl(l), c.ils));
-        return __fmul_rn(x, c.is);
+        if constexpr (C) x = __fadd_rn(x, U ? tofl(l) : __fmul_rn(tofl(l), c.ils));
+        return U ? x : __fmul_rn(x, c.is);
     }
     // four values at element e of a box whose residual box is lo_off bytes on
     __device__ static float4 ld4(const unsigned char* box, int e, int lo_off, const Sc& c)
@@ -108,10 +112,14 @@ struct Code {
     }
     __device__ static void enc(float v, const Sc& c, S& h, S& l)
     {
-        const float xs = __fmul_rn(v, c.s);
+        const float xs = U ? v : __fmul_rn(v, c.s);
         h = fromfl<S>(xs);
-        if constexpr (C) l = fromfl<S>(__fmul_rn(__fsub_rn(xs, tofl(h)), c.ls));
-        else l = h;
+        if constexpr (C) {
+            const float r = __fsub_rn(xs, tofl(h));
+            l = fromfl<S>(U ? r : __fmul_rn(r, c.ls));
+        } else {
+            l = h;
+        }
     }
     // encode four values, store them at padded index i (when st), return them decoded
     __device__ static float4 st4(float4 v, const Sc& c, void* hi, void* lo, long long i, bool st)
@@ -346,7 +354,20 @@ __global__ void __launch_bounds__(256) k_fused16(F16Args a, const __grid_constan
     float pxw = px_at(u0 - 3);
     int u_fail = u1 + 1;
 
-    for (int u = u0; u <= u1; ++u) {
+    // The x-interior iterations of a tile whose columns are all cells run a
+    // separately compiled body without the general path: iteration u is
+    // interior when plane u-3 and faces u-2 .. u-1 have alpha_x = 0 (px = 1),
+    // face u-2 has the 4th-order gradient and plane u-3 is an own plane.  Both
+    // bodies evaluate the same expressions there.
+    int fast_lo = u1 + 1, fast_hi = u1 + 1;
+    if (kfull && a.xi_hi > a.xi_lo) {
+        fast_lo = max(max(a.xi_lo + 3, 3), i_beg + 3);
+        fast_hi = min(min(a.xi_hi + 1, nx), u1 + 1);
+        if (fast_lo >= fast_hi) fast_lo = fast_hi = u1 + 1;
+    }
+
+    auto iteration = [&](const int u, auto fast_tag) -> bool {
+        constexpr bool FAST = decltype(fast_tag)::value;
         const int ps = pslot[3], vsg = vslot[0];
         const bool ok = mbar_wait(bar0 + 8u * ps, (pph >> ps) & 1u, a.wait_us) &&
                         mbar_wait(bar0 + 8u * (C::RING + vsg), (vph >> vsg) & 1u, a.wait_us);
@@ -359,33 +380,42 @@ __global__ void __launch_bounds__(256) k_fused16(F16Args a, const __grid_constan
         if (__syncthreads_or(!ok)) {
             if (tid == 0) atomicMin(a.status + kStatusTimeout, blockIdx.x + gridDim.x * blockIdx.y);
             u_fail = u;
-            break;
+            return false;
         }
         pph ^= 1u << ps;
         vph ^= 1u << vsg;
         if (tid == 0 && u + C::D <= u1) issue(u + C::D, pslot[C::RING - 1], vslot[C::VSTAGES - 1]);
-        const float ax_next = ax_at(u + 1), px_next = px_at(u - 2);
+        float ax_next = 0.0f, px_next = 1.0f;
+        if constexpr (!FAST) {
+            ax_next = ax_at(u + 1);
+            px_next = px_at(u - 2);
+        }
         const unsigned char* const vs = sm + C::VST0 + vsg * C::V_STAGE;
 
         pq0 = pq1; pq1 = pq2; pq2 = pq3;
         pq3 = K::ld4(pbox, cP, C::P_LO, a.sp);
 
         // ---- new Vx on face f = u-2 (planes u-3 .. u) ----
-        if (u >= i_beg) {
+        if (FAST || u >= i_beg) {
             const int f = u - 2;
             float4 vnew = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (f >= 0 && f <= nx - 2 && row_ok) {
+            if (FAST ? row_ok : (f >= 0 && f <= nx - 2 && row_ok)) {
                 const float4 vo = K::ld4(vs + C::VX_OFF, w * C::TK + 4 * lane, C::VX_LO, a.sv);
-                const bool fourth = (f > 0 && f < nx - 2);
-                const float axf = axw2, axf1 = axw1;
                 float4 v;
-                if (fourth && axf == 0.0f && axf1 == 0.0f && kfull) {
+                if constexpr (FAST) {
                     v = vel4m(cf, pq0, pq1, pq2, pq3, vo, dxi, 15, 15);
                 } else {
-                    float4 dm;
+                    const bool fourth = (f > 0 && f < nx - 2);
+                    const float axf = axw2, axf1 = axw1;
+                    if (fourth && axf == 0.0f && axf1 == 0.0f && kfull) {
+                        v = vel4m(cf, pq0, pq1, pq2, pq3, vo, dxi, 15, 15);
+                    } else {
+                        float4 dm;
 #pragma unroll
-                    for (int q = 0; q < 4; ++q) at4(dm, q) = damp(fmaxf(axf, at4(myz, q)), fmaxf(axf1, at4(myz, q)), cf.dt);
-                    v = vel4m(cf, pq0, pq1, pq2, pq3, vo, dm, fourth ? 15 : 0, okk);
+                        for (int q = 0; q < 4; ++q)
+                            at4(dm, q) = damp(fmaxf(axf, at4(myz, q)), fmaxf(axf1, at4(myz, q)), cf.dt);
+                        v = vel4m(cf, pq0, pq1, pq2, pq3, vo, dm, fourth ? 15 : 0, okk);
+                    }
                 }
                 vnew = K::st4(v, a.sv, a.vout_hi[0], a.vout_lo[0], f * PL + own,
                               f >= i_beg && f < i_end && st_ok);
@@ -395,13 +425,14 @@ __global__ void __launch_bounds__(256) k_fused16(F16Args a, const __grid_constan
 
         // ---- plane i = u-3: new Vy / Vz (with halos), then P^{n+1} ----
         const int i = u - 3;
-        if (i >= i_beg) {
-            const float axi = axw3;
-            const bool xint = (axi == 0.0f);
+        if (FAST || i >= i_beg) {
+            const float axi = FAST ? 0.0f : axw3;
+            const bool xint = FAST || (axi == 0.0f);
             const unsigned char* const pst = sm + C::RING0 + pslot[0] * C::P_STAGE;
             const unsigned char* const vys = vs + C::VY_OFF;
             const unsigned char* const vzs = vs + C::VZ_OFF;
             const long long ib = (long long)i * PL;
+            const float4 pown = pq0;   // own row of plane i
 
 #pragma unroll
             for (int m = 0; m < 2; ++m) {
@@ -414,11 +445,15 @@ __global__ void __launch_bounds__(256) k_fused16(F16Args a, const __grid_constan
                         const float4 pm = K::ld4(pst, r * C::PC + c, C::P_LO, a.sp);
                         const float4 p0 = K::ld4(pst, (r + 1) * C::PC + c, C::P_LO, a.sp);
                         const float4 p1 = K::ld4(pst, (r + 2) * C::PC + c, C::P_LO, a.sp);
-                        const float4 p2 = K::ld4(pst, (r + 3) * C::PC + c, C::P_LO, a.sp);
+                        // row r+3 of the box is the own row for the first item
+                        const float4 p2 = m == 0 ? pown : K::ld4(pst, (r + 3) * C::PC + c, C::P_LO, a.sp);
                         const float4 vo = K::ld4(vys, r * C::TK + 4 * lane, C::VY_LO, a.sv);
                         const bool fourth = (jf > 0 && jf < ny - 2);
                         float4 vv;
-                        if (fourth && xint && kfull) {
+                        if constexpr (FAST) {
+                            // the row's gradient order is uniform over its threads
+                            vv = vel4m(cf, pm, p0, p1, p2, vo, dyi[m], fourth ? 15 : 0, 15);
+                        } else if (fourth && xint && kfull) {
                             vv = vel4m(cf, pm, p0, p1, p2, vo, dyi[m], 15, 15);
                         } else {
                             float4 dm;
@@ -438,7 +473,6 @@ __global__ void __launch_bounds__(256) k_fused16(F16Args a, const __grid_constan
             }
 
             // Vz: own faces kb .. kb+3 of row jr
-            const float4 pown = pq0;
             {
                 float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (row_ok) {
@@ -498,15 +532,18 @@ __global__ void __launch_bounds__(256) k_fused16(F16Args a, const __grid_constan
                 const float2 za = *reinterpret_cast<const float2*>(zr + 2);
                 const float4 zb = *reinterpret_cast<const float4*>(zr + 4);
                 const float zc = zr[8];
-                float4 pd;
+                // px[i] = 1 on x-interior planes, so min(px[i], min(py, pz)) = mpz there
+                float4 pd = mpz;
+                if constexpr (!FAST) {
 #pragma unroll
-                for (int q = 0; q < 4; ++q) at4(pd, q) = fminf(pxw, at4(mpz, q));
+                    for (int q = 0; q < 4; ++q) at4(pd, q) = fminf(pxw, at4(mpz, q));
+                }
                 float4 out;
                 out.x = pup(cf, pown.x, qx2.x, qx1.x, qx3.x, qx0.x, yp.x, ym.x, ypp.x, ymm.x, zb.x, za.y, zb.y, za.x, pd.x);
                 out.y = pup(cf, pown.y, qx2.y, qx1.y, qx3.y, qx0.y, yp.y, ym.y, ypp.y, ymm.y, zb.y, zb.x, zb.z, za.y, pd.y);
                 out.z = pup(cf, pown.z, qx2.z, qx1.z, qx3.z, qx0.z, yp.z, ym.z, ypp.z, ymm.z, zb.z, zb.y, zb.w, zb.x, pd.z);
                 out.w = pup(cf, pown.w, qx2.w, qx1.w, qx3.w, qx0.w, yp.w, ym.w, ypp.w, ymm.w, zb.w, zb.z, zc, zb.y, pd.w);
-                if (!kfull) {
+                if (!FAST && !kfull) {
 #pragma unroll
                     for (int q = 0; q < 4; ++q)
                         if (kb + q >= nz) at4(out, q) = 0.0f;
@@ -515,8 +552,10 @@ __global__ void __launch_bounds__(256) k_fused16(F16Args a, const __grid_constan
             }
         }
 
-        axw3 = axw2; axw2 = axw1; axw1 = axw0; axw0 = ax_next;
-        pxw = px_next;
+        if constexpr (!FAST) {
+            axw3 = axw2; axw2 = axw1; axw1 = axw0; axw0 = ax_next;
+            pxw = px_next;
+        }
         {
             const int pfree = pslot[0];
 #pragma unroll
@@ -527,6 +566,22 @@ __global__ void __launch_bounds__(256) k_fused16(F16Args a, const __grid_constan
             for (int q = 0; q + 1 < C::VSTAGES; ++q) vslot[q] = vslot[q + 1];
             vslot[C::VSTAGES - 1] = vfree;
         }
+        return true;
+    };
+
+    for (int u = u0; u <= u1;) {
+        if (u == fast_lo) {
+            bool ran = true;
+            for (; u < fast_hi; ++u)
+                if (!iteration(u, std::true_type{})) { ran = false; break; }
+            if (!ran) break;
+            // the alpha_x / px window of the general iterations that follow
+            axw3 = ax_at(u - 3); axw2 = ax_at(u - 2); axw1 = ax_at(u - 1); axw0 = ax_at(u);
+            pxw = px_at(u - 3);
+            continue;
+        }
+        if (!iteration(u, std::false_type{})) break;
+        ++u;
     }
 
     // after a timed-out wait, the copies of iterations u_fail .. u_fail+D-1 may

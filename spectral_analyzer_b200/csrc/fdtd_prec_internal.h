@@ -170,6 +170,7 @@ struct F16Args {
     double* rec_out;
     unsigned* status;              // kStatusTimeout is set when a load wait runs out
     unsigned wait_us;
+    int xi_lo, xi_hi;              // planes [xi_lo, xi_hi) have alpha_x = 0 (empty: none)
 };
 
 struct F16Cache;                   // host-side tensor maps of a handle's 16-bit fields

@@ -259,6 +259,7 @@ struct FdtdB200Prec {
     // The single-pass 16-bit step writes the other velocity set (v2) and
     // flips vset; the two-pass step updates the current set in place.
     int kernel = 0;             // 1: single-pass step (16-bit modes), 0: two-pass
+    int xi_lo = 0, xi_hi = 0;   // planes with alpha_x = 0 (the single pass's interior body)
     Field v2[3] = {};
     int vset = 0;
     F16Cache* maps = nullptr;
@@ -424,6 +425,8 @@ int fused16_step(FdtdB200Prec* p)
     }
     a.status = p->d_status;
     a.wait_us = kWaitUs;
+    a.xi_lo = p->xi_lo;
+    a.xi_hi = p->xi_hi;
     const void* bases[8] = {P.hi, P.lo, vin[0].hi, vin[0].lo, vin[1].hi, vin[1].lo, vin[2].hi, vin[2].lo};
     PCK(launch_fused16(p->mode, a, p->maps, bases, p->stream));
     ++p->launches;
@@ -526,6 +529,7 @@ FdtdB200Prec* fdtd_b200_prec_create(int Nx, int Ny, int Nz, double dx, double c,
     std::vector<double> t64;
     build<float>(p, (float)dx, (float)c, (float)rho_air, 0.77f, 1.732050808f, n_pml, a6, t32, p->cf32);
     build<double>(p, dx, c, rho_air, 0.77, 1.732050808, n_pml, a6, t64, p->cf64);
+    x_interior_run(t32.data(), Nx, &p->xi_lo, &p->xi_hi);
     p->dt = mode == kFP64 ? p->cf64.dt : (double)p->cf32.dt;
     const size_t tb = mode == kFP64 ? t64.size() * 8 : t32.size() * 4;
     bool ok = cudaMalloc(&p->d_tab, tb) == cudaSuccess &&
@@ -537,6 +541,7 @@ FdtdB200Prec* fdtd_b200_prec_create(int Nx, int Ny, int Nz, double dx, double c,
     const bool fp16 = (mode == kFP16 || mode == kFP16C);
     for (int q = 0; q < 5 && ok; ++q) {
         Field& f = p->f[q];
+        // BF16 forms are stored unscaled (the single-pass kernel relies on it)
         f.scale = fp16 ? (q < 2 ? p_scale : v_scale) : 1.0f;
         f.inv_scale = 1.0f / f.scale;
         f.lo_scale = mode == kFP16C ? 2048.0f : 1.0f;   // keeps half residuals out of subnormals
