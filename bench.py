@@ -70,6 +70,8 @@ def parse_args():
                     help="storage-precision study (FP32/BF16/FP16, compensated) vs an FP64 GPU run")
     ap.add_argument("--precision-steps", type=int, default=10000)
     ap.add_argument("--precision-audit", type=int, default=500)
+    ap.add_argument("--precision-time-steps", type=int, default=300,
+                    help="steps timed per 16-bit mode and step kernel (0: no timing)")
     ap.add_argument("--adjoint", action="store_true",
                     help="gradient w.r.t. per-cell absorption: adjoint timing and checks")
     ap.add_argument("--adjoint-steps", type=int, default=4000)
@@ -469,9 +471,45 @@ def serve_arm(args):
     return 0 if same else 1
 
 
+def precision_timing(room, steps: int, warmup: int = 20) -> dict:
+    """Device time per step of each 16-bit storage mode on both step kernels
+    (CUDA events on the handle's stream, no audits), with the single pass's
+    roofline on the mode's algorithmic bytes: one read and one write of the
+    four fields, 2 B per value plain and 4 B compensated."""
+    import torch
+    from spectral_analyzer_b200.precision import BYTES_PER_VALUE, PrecisionRoom
+    peak, peak_kind = measured_peak()
+    out = {}
+    for mode in ("bf16", "fp16", "bf16c", "fp16c"):
+        row = {"bytes_per_update": 8 * BYTES_PER_VALUE[mode]}
+        for kern in ("fused", "two_pass"):
+            pr = PrecisionRoom(room, mode, kernel=kern, trace_capacity=steps + warmup + 4, audit_capacity=1)
+            pr.step(warmup)
+            torch.cuda.synchronize()
+            s = pr.torch_stream()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            l0 = pr.launch_count
+            e0.record(s)
+            pr.step(steps)
+            e1.record(s)
+            torch.cuda.synchronize()
+            ms = e0.elapsed_time(e1) / steps
+            g = room.cells / ms / 1e6
+            row[kern] = {"ms_per_step": ms, "gcell_updates_per_s": g, "launches": pr.launch_count - l0}
+            pr.close()
+        g = row["fused"]["gcell_updates_per_s"]
+        achieved = g * row["bytes_per_update"]
+        row["roofline_fused"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                                 "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs"}
+        out[mode] = row
+    return out
+
+
 def precision_arm(args):
     """Storage precision on the 512x384x256 room: traces and energy audit of each
-    storage mode against the FP64 GPU oracle run of the same room."""
+    storage mode against the FP64 GPU oracle run of the same room, and the
+    device time per step of the 16-bit modes on the single-pass and two-pass
+    step kernels."""
     import torch
     from spectral_analyzer_b200.precision import study
     from spectral_analyzer_b200.rooms import large_room, seeded_room
@@ -488,10 +526,13 @@ def precision_arm(args):
             "config": {"workload": f"room{room.nx}x{room.ny}x{room.nz}_ricker_storage_precision",
                        "steps": room.n_steps, "receivers": len(room.receivers),
                        "audit_every": args.precision_audit,
-                       "kernel": "two-pass, templated on storage (fdtd_precision.cu)"},
+                       "kernel": "16-bit modes: single-pass TMA step (fdtd_fused16.cu), two-pass on "
+                                 "audit steps; FP32/FP64: two-pass (fdtd_precision.cu)"},
             "fp64_oracle": {k: v for k, v in res["fp64"].items() if k != "energy"},
             "energy_fp64": res["fp64"]["energy"],
             "modes": rows}
+    if args.precision_time_steps > 0:
+        line["step_time_16bit"] = precision_timing(room, args.precision_time_steps)
     print(json.dumps(line), flush=True)
     return 0
 
