@@ -60,6 +60,32 @@ def test_batch_equals_alone(cuda, use_graph, tile_k):
         assert bits_equal(f.get_velocity_z(), Vz)
 
 
+def test_batch_matches_the_oracle(cuda):
+    """Each room of the mixed batch against the oracle directly (not only
+    against the single-room engine): traces and final fields bit for bit."""
+    from oracle import OracleFDTD
+    from spectral_analyzer_b200.serving import EngineBatch, make_solver
+    rs = rooms()
+    solvers = [make_solver(r) for r in rs]
+    b = EngineBatch()
+    b.set(solvers, [r.n_steps for r in rs])
+    while any(f.step_count < r.n_steps for f, r in zip(solvers, rs)):
+        b.step(41, True)
+        _, status = b.sync()
+        assert not status.any()
+    b.set([], [])
+    for r, f in zip(rs, solvers):
+        o = OracleFDTD(r.nx, r.ny, r.nz, r.dx, r.c, r.rho, n_pml=r.n_pml)
+        o.set_face_absorption(r.absorption)
+        idx, w = o.precompute_pressure_samplers(r.receiver_xyz())
+        tro = o.run(r.n_steps, r.src_flat, r.signal(), idx, w)
+        got = f.get_traces()
+        assert bits_equal(got, tro), (r.describe(), first_mismatch(got, tro))
+        assert bits_equal(f.get_pressure_field(), o.get_pressure_field()), r.describe()
+        assert bits_equal(f.get_velocity_x(), o.get_velocity_x()), r.describe()
+        del o
+
+
 def test_members_join_and_leave(cuda):
     """Rooms enter mid-run and continue on the single-room path after leaving."""
     from spectral_analyzer_b200.serving import EngineBatch, make_solver
