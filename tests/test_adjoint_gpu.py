@@ -119,7 +119,7 @@ def test_autograd_function(cuda):
     r2.set_absorption(prob.a)
     y = r2.forward()
     g = r2.backward(2.0 * (y - tgt))
-    assert float(loss) == pytest.approx(float(np.sum((y - tgt) ** 2)), rel=1e-12)
+    assert float(loss.detach()) == pytest.approx(float(np.sum((y - tgt) ** 2)), rel=1e-12)
     assert a.grad.dtype == torch.float32
     assert np.array_equal(a.grad.cpu().numpy(), g.astype(np.float32))
     assert r.launch_count > 0
