@@ -224,9 +224,12 @@ FDTD_B200_API int fdtd_b200_step_async(AcousticFDTDState* st, int n_steps);
  * by an async step) or FDTD_ERR_CUDA.  Clears the latch. */
 FDTD_B200_API int fdtd_b200_synchronize(AcousticFDTDState* st);
 
-/* Step-kernel selection: 0 automatic (fused single pass for open rooms,
- * two-pass otherwise), 1 two-pass, 2 fused (rejected with FDTD_ERR_ARG when
- * the scene has walls, fractions or an active plate). */
+/* Step-kernel selection: 0 automatic (fused single pass for open rooms and
+ * for walled scenes of at least 2^24 cells, two-pass for smaller walled
+ * scenes), 1 two-pass, 2 fused.  Walled scenes (solid cells, face fractions,
+ * an active plate) run the single pass with the walled rules; both kernels
+ * give the same results bit for bit.  FDTD_ERR_ARG for 2 when the row
+ * padding does not allow the single pass. */
 FDTD_B200_API int fdtd_b200_set_kernel(AcousticFDTDState* st, int mode);
 FDTD_B200_API int fdtd_b200_get_kernel(const AcousticFDTDState* st);
 

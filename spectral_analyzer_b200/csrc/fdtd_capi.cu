@@ -111,6 +111,10 @@ struct AcousticFDTDState {
     long long* d_below = nullptr;
     long long* d_vzb = nullptr;
     long long* d_vza = nullptr;
+    // four-cell groups whose divergence reads a plate face (padded index of the
+    // group's first cell): recomputed after a walled single-pass step
+    long long* d_pfix = nullptr;
+    int n_pfix = 0;
     std::vector<int> h_act;
     float* d_w[3] = {nullptr, nullptr, nullptr};
     int wi_cur = 0, wi_prev = 1, wi_tmp = 2;
@@ -455,10 +459,25 @@ bool fused_eligible(const AcousticFDTDState* st)
            fused_supported(st->g);
 }
 
+// A walled scene (solid cells, face fractions or an active plate) that the
+// single-pass step can take: whole room, row padding as the TMA maps need.
+bool fused_walled_ok(const AcousticFDTDState* st)
+{
+    return (st->any_solid || st->d_frac[0] || st->n_act > 0) && fused_supported(st->g);
+}
+
+// Walled scenes take the single pass automatically from this many cells on:
+// below it the fields stay in L2 and the two-pass kernels are as fast or
+// faster (170x140x74: 49 against 68 us per step; 256x200x128: 120 against
+// 117; 512x384x256: 825 against 655).
+constexpr long long kWalledFusedCells = 1LL << 24;
+
 bool use_fused(const AcousticFDTDState* st)
 {
     if (st->kernel_mode == 1) return false;
-    return fused_eligible(st);
+    if (fused_eligible(st)) return true;
+    if (!fused_walled_ok(st)) return false;
+    return st->kernel_mode == 2 || (long long)st->N >= kWalledFusedCells;
 }
 
 int prof_begin(AcousticFDTDState* st, cudaEvent_t* e1)
@@ -617,6 +636,12 @@ int one_step(AcousticFDTDState* st, bool sync_check, bool defer_record = false)
                     st->d_status};
         a.hold_plane = st->hold_plane;
         a.wait_us = st->wait_us;
+        const bool walled = !fused_eligible(st);
+        if (walled) {
+            for (int c2 = 0; c2 < 3; ++c2) a.fr[c2] = st->d_frac[c2];
+            a.frac_div = st->has_frac;
+            a.solid = st->d_solid;
+        }
         if (fuse_deposit) {
             const long long c = st->ps.idx[0], t = c / st->g.sz;
             a.dep_sig = st->d_ps_sig;
@@ -635,6 +660,18 @@ int one_step(AcousticFDTDState* st, bool sync_check, bool defer_record = false)
         CK(launch_fused_step(a, st->fcache, s));
         ++st->launches;
         st->cv ^= 1;
+        if (walled && st->n_act > 0) {
+            // the plate sets its faces' velocity after the update (as on the
+            // two-pass path); the cells whose divergence reads those faces are
+            // then updated again from P^n and the new velocities
+            CK(launch_plate_inject(st->n_act, st->d_act, st->d_vzb, st->d_vza, st->d_w[st->wi_cur],
+                                   st->d_w[st->wi_prev], st->cf.inv_dt, st->V(2), s));
+            const bool hf = st->has_frac;
+            CK(launch_pressure_groups(st->g, st->cf, st->tb, st->P(), st->Pn(), st->V(0), st->V(1), st->V(2),
+                                      hf ? st->d_frac[0] : nullptr, hf ? st->d_frac[1] : nullptr,
+                                      hf ? st->d_frac[2] : nullptr, st->d_solid, st->d_pfix, st->n_pfix, s));
+            st->launches += 2;
+        }
         if ((rc = prof_end(st, e1, fused_kernel_launches_per_step()))) return rc;
     } else {
         CK(launch_velocity_general(st->g, st->cf, st->tb, st->P(), st->V(0), st->V(1), st->V(2),
@@ -704,7 +741,7 @@ void free_state(AcousticFDTDState* st)
     cudaFree(st->d_solid);
     for (int c = 0; c < 3; ++c) { cudaFree(st->d_frac[c]); cudaFree(st->d_w[c]); }
     cudaFree(st->d_act); cudaFree(st->d_nb13); cudaFree(st->d_above); cudaFree(st->d_below);
-    cudaFree(st->d_vzb); cudaFree(st->d_vza); cudaFree(st->d_ext); cudaFree(st->d_slice);
+    cudaFree(st->d_vzb); cudaFree(st->d_vza); cudaFree(st->d_pfix); cudaFree(st->d_ext); cudaFree(st->d_slice);
     cudaFreeHost(st->h_ext);
     cudaFree(st->d_ps_sig);
     cudaFree(st->d_rec_idx); cudaFree(st->d_rec_w); cudaFree(st->d_trace);
@@ -891,6 +928,23 @@ AcousticFDTDState* create_impl(int Nx, int Ny, int Nz, float dx, float c, float 
             CKN(cudaMemcpy(st->d_below, below.data(), na * sizeof(long long), cudaMemcpyHostToDevice));
             CKN(cudaMemcpy(st->d_vzb, vzb.data(), na * sizeof(long long), cudaMemcpyHostToDevice));
             CKN(cudaMemcpy(st->d_vza, vza.data(), na * sizeof(long long), cudaMemcpyHostToDevice));
+            // cells whose pressure update reads plate face kf: k = kf-1 .. kf+2
+            std::vector<long long> fix;
+            for (const auto* lst : {&vzb, &vza})
+                for (long long q : *lst) {
+                    if (q < 0) continue;
+                    const int kf = (int)(q % st->g.sz);
+                    const long long row = q - kf;
+                    for (int k = kf - 1; k <= kf + 2; ++k)
+                        if (k >= 0 && k < Nz) fix.push_back(row + (k & ~3));
+                }
+            std::sort(fix.begin(), fix.end());
+            fix.erase(std::unique(fix.begin(), fix.end()), fix.end());
+            st->n_pfix = (int)fix.size();
+            if (st->n_pfix > 0) {
+                CKN(cudaMalloc(&st->d_pfix, fix.size() * sizeof(long long)));
+                CKN(cudaMemcpy(st->d_pfix, fix.data(), fix.size() * sizeof(long long), cudaMemcpyHostToDevice));
+            }
         }
     }
 
@@ -1389,7 +1443,7 @@ int fdtd_b200_set_kernel(AcousticFDTDState* st, int mode)
 {
     if (!st) return FDTD_ERR_NULL;
     if (mode < 0 || mode > 2) return FDTD_ERR_ARG;
-    if (mode == 2 && !fused_eligible(st)) return FDTD_ERR_ARG;
+    if (mode == 2 && !fused_eligible(st) && !fused_walled_ok(st)) return FDTD_ERR_ARG;
     st->kernel_mode = mode;
     return FDTD_OK;
 }

@@ -1,5 +1,6 @@
 /*
- * fdtd_fused.cu — single-pass velocity+pressure step for open rooms.
+ * fdtd_fused.cu — single-pass velocity+pressure step for open rooms (and, with
+ * the walled rules of the two-pass kernels, for large walled scenes).
  *
  * One launch advances V^{n-1/2} -> V^{n+1/2} and P^n -> P^{n+1} over the whole
  * grid, reading each field once and writing each once: 16 B read + 16 B
@@ -103,6 +104,20 @@ __device__ __forceinline__ float4 lds4(const float* p) { return *reinterpret_cas
 __device__ __forceinline__ void sts4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 __device__ __forceinline__ void stg4(float* p, float4 v) { *reinterpret_cast<float4*>(p) = v; }
 __device__ __forceinline__ float& at(float4& v, int q) { return reinterpret_cast<float*>(&v)[q]; }
+__device__ __forceinline__ float4 ldg4(const float* p) { return __ldg(reinterpret_cast<const float4*>(p)); }
+// a face whose open fraction is 0 is closed
+__device__ __forceinline__ float4 close4(float4 v, const float4& fr)
+{
+    if (fr.x == 0.0f) v.x = 0.0f;
+    if (fr.y == 0.0f) v.y = 0.0f;
+    if (fr.z == 0.0f) v.z = 0.0f;
+    if (fr.w == 0.0f) v.w = 0.0f;
+    return v;
+}
+__device__ __forceinline__ float4 mul4(const float4& v, const float4& fr)
+{
+    return make_float4(fmul(v.x, fr.x), fmul(v.y, fr.y), fmul(v.z, fr.z), fmul(v.w, fr.w));
+}
 
 // staggered gradient: 4th order in the interior of the face range, else 2nd
 __device__ __forceinline__ float grad4(const Coef& cf, float pm, float p0, float p1, float p2, bool fourth)
@@ -217,8 +232,12 @@ __device__ __forceinline__ void init_barriers(unsigned bar0)
 // One tile (TJ x TK columns, planes [seg*seg_len, ...)) of the fused step.
 // Returns false when a load wait ran out (the CTA must stop; status is set).
 // PEER = false compiles out the neighbour ghost-plane stores (single rooms and
-// batches), which the slab step of a split room needs.
-template <class C, bool PEER = true>
+// batches), which the slab step of a split room needs.  WALLS = true adds the
+// walled-scene rules of the two-pass kernels to the general body: a face whose
+// open fraction is 0 is closed (its new velocity is 0), the divergence sees
+// each face's velocity times its fraction (when fractions were set), and
+// solid cells keep P = 0; the interior body is not used.
+template <class C, bool PEER = true, bool WALLS = false>
 __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap* tmP,
                                            const CUtensorMap* tmX, const CUtensorMap* tmY,
                                            const CUtensorMap* tmZ, int tile, int seg, int seg_len,
@@ -362,7 +381,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
     // evaluate the same expressions (alpha_x = 0, px = 1 there), so the results
     // do not depend on the choice.  The step runs in one wave, so a CTA left on
     // the general body for its whole march would set the kernel's time.
-    const bool clean = kfull;
+    const bool clean = kfull && !WALLS;
     int fast_lo = u1 + 1, fast_hi = u1 + 1;
     if (clean && a.tb.xi_hi > a.tb.xi_lo) {
         fast_lo = max(max(a.tb.xi_lo + 3, 3 - xg0), i_beg + 3);
@@ -378,6 +397,34 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
         // timeout is made by the whole CTA (the barrier below is also the one that
         // separates the previous iteration's reads from this iteration's writes)
         const int ps = pslot[3], vsg = vslot[0];
+        // WALLS: this iteration's face fractions and solid flags, loaded before
+        // the wait so that their latency overlaps it (they do not depend on it)
+        float4 pf_x = make_float4(1.f, 1.f, 1.f, 1.f), pf_y0 = pf_x, pf_y1 = pf_x, pf_z = pf_x;
+        float pf_h = 1.0f;
+        unsigned pf_s = 0u;
+        if constexpr (WALLS) {
+            const int f = u - 2, i = u - 3;
+            if (a.fr[0] && st_ok && u >= i_beg && f >= 0 && f <= nx - 2) pf_x = ldg4(a.fr[0] + f * PL + own);
+            if (i >= i_beg) {
+                const long long ib = (long long)i * PL;
+                if (a.fr[1] && kb < sz) {
+                    const int jf0 = j0 - 2 + w, jf1 = j0 - 2 + C::TJ + w;
+                    if (jf0 >= 0 && jf0 <= ny - 2) pf_y0 = ldg4(a.fr[1] + ib + (long long)jf0 * sz + kb);
+                    if (C::TJ + w < C::VYR && jf1 >= 0 && jf1 <= ny - 2)
+                        pf_y1 = ldg4(a.fr[1] + ib + (long long)jf1 * sz + kb);
+                }
+                if (a.fr[2] && st_ok) pf_z = ldg4(a.fr[2] + ib + own);
+                const int hl = tid - (C::NT - 32 * C::HW);
+                if (a.fr[2] && hl >= 0 && hl < 3 * C::TJ) {
+                    const int jl = hl / 3, which = hl - 3 * jl;
+                    const int kf = k0 - 4 + (which < 2 ? 2 + which : C::TK + 4);
+                    if (j0 + jl < ny && kf >= 0 && kf <= nz - 2)
+                        pf_h = __ldg(a.fr[2] + ib + (long long)(j0 + jl) * sz + kf);
+                }
+                if (a.solid && row_ok && kb < sz)
+                    pf_s = __ldg(reinterpret_cast<const unsigned*>(a.solid + ib + own));
+            }
+        }
         const bool ok = mbar_wait(bar0 + 8u * ps, (pph >> ps) & 1u, a.wait_us) &&
                         mbar_wait(bar0 + 8u * (C::RING + vsg), (vph >> vsg) & 1u, a.wait_us);
         // the source deposit, on the arriving plane's shared copy before anyone reads it
@@ -411,6 +458,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
         if (FAST || u >= i_beg) {
             const int f = u - 2, fg = f + xg0;
             float4 vnew = make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 vdiv = vnew;   // WALLS: the value the divergence sees
             if (FAST ? row_ok : (fg >= 0 && fg <= nxg - 2 && row_ok)) {
                 const float4 pm = lds4(smem + C::RING0 + pslot[0] * C::P_STAGE + cP);
                 const float4 p0 = lds4(smem + C::RING0 + pslot[1] * C::P_STAGE + cP);
@@ -436,6 +484,14 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                         vnew = vel4_general(cf, pm, p0, p1, p2, vo, aL, aR, fourth ? 15 : 0, okx);
                     }
                 }
+                if constexpr (WALLS) {
+                    vdiv = vnew;
+                    if (a.fr[0] && st_ok) {
+                        const float4 fr = pf_x;
+                        vnew = close4(vnew, fr);
+                        vdiv = a.frac_div ? mul4(vnew, fr) : vnew;
+                    }
+                }
                 if (f >= i_beg && f < i_end && st_ok) {
                     stg4(a.vout[0] + f * PL + own, vnew);
 #pragma unroll
@@ -444,7 +500,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                             stg4(a.pr.vx[sd] + (f + a.pr.dl[sd]) * PL + own, vnew);
                 }
             }
-            qx0 = qx1; qx1 = qx2; qx2 = qx3; qx3 = vnew;
+            qx0 = qx1; qx1 = qx2; qx2 = qx3; qx3 = WALLS ? vdiv : vnew;
         }
 
         // ---- plane i = u-3: new Vy / Vz (with halos), then P^{n+1} ----
@@ -491,8 +547,18 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                                     v = vel4_general(cf, pm, p0, p1, p2, vo, aL, aR, fourth ? 15 : 0, oky);
                                 }
                             }
+                            float4 fry = make_float4(1.f, 1.f, 1.f, 1.f);
+                            if constexpr (WALLS) {
+                                if (a.fr[1] && kb < sz) {
+                                    fry = m == 0 ? pf_y0 : pf_y1;
+                                    v = close4(v, fry);
+                                }
+                            }
                             if (r >= 2 && r < C::TJ + 2 && (FAST || kb < sz))
                                 stg4(a.vout[1] + ib + (long long)jf * sz + kb, v);
+                            if constexpr (WALLS) {
+                                if (a.fr[1] && a.frac_div && kb < sz) v = mul4(v, fry);
+                            }
                         }
                         sts4(vyn + r * C::TK + 4 * lane, v);
                     }
@@ -525,7 +591,17 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                             }
                             v = vel4_general(cf, pm, pown, p1, p2, vo, aL, aR, zm4, zok);
                         }
+                        float4 frz = make_float4(1.f, 1.f, 1.f, 1.f);
+                        if constexpr (WALLS) {
+                            if (a.fr[2] && st_ok) {
+                                frz = pf_z;
+                                v = close4(v, frz);
+                            }
+                        }
                         if (st_ok) stg4(a.vout[2] + ib + own, v);
+                        if constexpr (WALLS) {
+                            if (a.fr[2] && a.frac_div && st_ok) v = mul4(v, frz);
+                        }
                     }
                     sts4(vzn + w * C::PC + 4 * lane + 4, v);
                 }
@@ -545,6 +621,13 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                         const float dmp = face_damp(fmaxf(fmaxf(axi, ay), az_s[ch]),
                                                     fmaxf(fmaxf(axi, ay), az_s[ch + 1]), cf.dt);
                         vh = vupd(cf, vzs[jl * C::PC + ch], gr, dmp);
+                        if constexpr (WALLS) {
+                            if (a.fr[2]) {
+                                const float fz = pf_h;
+                                if (fz == 0.0f) vh = 0.0f;
+                                if (a.frac_div) vh = fmul(vh, fz);
+                            }
+                        }
                     }
                     vzn[jl * C::PC + ch] = vh;
                 }
@@ -575,6 +658,14 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
 #pragma unroll
                         for (int q = 0; q < 4; ++q)
                             if (kb + q >= nz) at(out, q) = 0.0f;
+                    }
+                    if constexpr (WALLS) {
+                        if (a.solid && kb < sz) {   // solid cells keep P = 0
+                            const unsigned sol = pf_s;
+#pragma unroll
+                            for (int q = 0; q < 4; ++q)
+                                if ((sol >> (8 * q)) & 0xFFu) at(out, q) = 0.0f;
+                        }
                     }
                     if (kb < sz) {
                         stg4(a.pn + ib + own, out);
@@ -639,7 +730,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
 }
 
 // Single-room step: one CTA per (tile, segment).
-template <class C, bool PEER>
+template <class C, bool PEER, bool WALLS = false>
 __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
                                                       const __grid_constant__ CUtensorMap tmP,
                                                       const __grid_constant__ CUtensorMap tmX,
@@ -659,8 +750,8 @@ __global__ void __launch_bounds__(C::NT) k_fused_step(FusedArgs a,
     init_barriers<C>(bar0);
     Pipe<C> pp;
     pp.init();
-    fused_tile<C, PEER>(a, &tmP, &tmX, &tmY, &tmZ, blockIdx.x, blockIdx.y, seg_len, tiles_k, smem, sbase,
-                        bar0, pp);
+    fused_tile<C, PEER, WALLS>(a, &tmP, &tmX, &tmY, &tmZ, blockIdx.x, blockIdx.y, seg_len, tiles_k, smem,
+                               sbase, bar0, pp);
 }
 
 
@@ -860,11 +951,19 @@ static cudaError_t launch_step_of(const FusedArgs& a, FusedCache* cache, cudaStr
         e = cudaFuncSetAttribute(k_fused_step<C, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)C::SMEM_BYTES);
         if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(k_fused_step<C, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)C::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
         e = cudaDeviceGetAttribute(&g_sms[shape][dev], cudaDevAttrMultiProcessorCount, dev);
         if (e != cudaSuccess) return e;
         int slots = 0;
         e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&slots, k_fused_step<C, true>, C::NT, C::SMEM_BYTES);
         if (e != cudaSuccess) return e;
+        int slots_w = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&slots_w, k_fused_step<C, false, true>, C::NT,
+                                                          C::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        slots = slots < slots_w ? slots : slots_w;
         g_slots_per_sm[shape][dev] = slots > 0 ? slots : 1;
         g_configured[shape][dev] = true;
     }
@@ -889,7 +988,12 @@ static cudaError_t launch_step_of(const FusedArgs& a, FusedCache* cache, cudaStr
     segs = (n_own + seg_len - 1) / seg_len;
     dim3 grid((unsigned)tiles, (unsigned)segs, 1);
     const bool peer = a.pr.pn[0] || a.pr.pn[1] || a.pr.vx[0] || a.pr.vx[1];
-    if (peer)
+    const bool walls = a.fr[0] || a.fr[1] || a.fr[2] || a.solid;
+    if (walls && (peer || a.xs.nxg > 0)) return cudaErrorInvalidValue;   // walled scenes are whole rooms
+    if (walls)
+        k_fused_step<C, false, true><<<grid, C::NT, C::SMEM_BYTES, s>>>(a, maps[0], maps[1], maps[2], maps[3],
+                                                                        seg_len, tiles_k);
+    else if (peer)
         k_fused_step<C, true><<<grid, C::NT, C::SMEM_BYTES, s>>>(a, maps[0], maps[1], maps[2], maps[3], seg_len,
                                                                  tiles_k);
     else

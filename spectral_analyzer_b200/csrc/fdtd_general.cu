@@ -127,18 +127,15 @@ __global__ void __launch_bounds__(256) k_velocity_general(
     }
 }
 
-// Pressure update from the 4th-order divergence (acoustic_fdtd.cpp:894-952,
-// :1176-1234).  Faces outside the grid read as zero; with fractions each face
-// is scaled by its open fraction; solid cells are skipped (they stay zero in
-// both pressure buffers, so the thread writes zero there).
-__global__ void __launch_bounds__(256) k_pressure_general(
-    Grid g, Coef cf, Tables tb, const float* __restrict__ p, float* __restrict__ pn,
-    const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz,
-    const float* __restrict__ fx, const float* __restrict__ fy, const float* __restrict__ fz,
-    const uint8_t* __restrict__ solid, const unsigned* __restrict__ gate)
+// The pressure update of cells k0 .. k0+3 of row (i, j), id = their padded index.
+__device__ __forceinline__ void pressure_cells4(const Grid& g, const Coef& cf, const Tables& tb,
+                                                const float* __restrict__ p, float* __restrict__ pn,
+                                                const float* __restrict__ vx, const float* __restrict__ vy,
+                                                const float* __restrict__ vz, const float* __restrict__ fx,
+                                                const float* __restrict__ fy, const float* __restrict__ fz,
+                                                const uint8_t* __restrict__ solid, int i, int j, int k0,
+                                                long long id)
 {
-    GEN_INDEX
-    if (gate && gate[kStatusPlate] != 0xFFFFFFFFu) return;   // this step's plate update failed
     const long long P = g.plane, S = g.sz;
     // face values times their fractions, four cells at a time (zero when absent)
     auto face4 = [&](const float* v, const float* f, long long q, bool exists, float (&out)[4]) {
@@ -191,6 +188,39 @@ __global__ void __launch_bounds__(256) k_pressure_general(
         out[q] = fmul(fsub(pc[q], fmul(cf.bulk, dv)), fminf(pxy, __ldg(tb.pz + k)));
     }
     st4(pn, id, out);
+}
+
+// Pressure update from the 4th-order divergence (acoustic_fdtd.cpp:894-952,
+// :1176-1234).  Faces outside the grid read as zero; with fractions each face
+// is scaled by its open fraction; solid cells are skipped (they stay zero in
+// both pressure buffers, so the thread writes zero there).
+__global__ void __launch_bounds__(256) k_pressure_general(
+    Grid g, Coef cf, Tables tb, const float* __restrict__ p, float* __restrict__ pn,
+    const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz,
+    const float* __restrict__ fx, const float* __restrict__ fy, const float* __restrict__ fz,
+    const uint8_t* __restrict__ solid, const unsigned* __restrict__ gate)
+{
+    GEN_INDEX
+    if (gate && gate[kStatusPlate] != 0xFFFFFFFFu) return;   // this step's plate update failed
+    pressure_cells4(g, cf, tb, p, pn, vx, vy, vz, fx, fy, fz, solid, i, j, k0, id);
+}
+
+// The same update on a list of four-cell groups (padded index of each group's
+// first cell): after the single-pass walled step, the cells whose divergence
+// reads a plate face, recomputed once the plate has set those faces.
+__global__ void __launch_bounds__(256) k_pressure_groups(
+    Grid g, Coef cf, Tables tb, const float* __restrict__ p, float* __restrict__ pn,
+    const float* __restrict__ vx, const float* __restrict__ vy, const float* __restrict__ vz,
+    const float* __restrict__ fx, const float* __restrict__ fy, const float* __restrict__ fz,
+    const uint8_t* __restrict__ solid, const long long* __restrict__ groups, int n_groups)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n_groups) return;
+    const long long id = groups[t];
+    const int i = (int)(id / g.plane);
+    const long long r = id - (long long)i * g.plane;
+    const int j = (int)(r / g.sz), k0 = (int)(r - (long long)j * g.sz);
+    pressure_cells4(g, cf, tb, p, pn, vx, vy, vz, fx, fy, fz, solid, i, j, k0, id);
 }
 
 // Kirchhoff plate step (acoustic_fdtd.cpp:984-1053), one thread per active node.
@@ -343,6 +373,17 @@ cudaError_t launch_plate_step(int n_act, const int* act, const int* nb13, const 
     if (n_act <= 0) return cudaSuccess;
     k_plate_step<<<(n_act + 127) / 128, 128, 0, s>>>(n_act, act, nb13, above, below, w, wp, wt,
                                                      ext, p, pc, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_pressure_groups(const Grid& g, const Coef& cf, const Tables& tb, const float* p, float* pn,
+                                   const float* vx, const float* vy, const float* vz, const float* fx,
+                                   const float* fy, const float* fz, const uint8_t* solid,
+                                   const long long* groups, int n_groups, cudaStream_t s)
+{
+    if (n_groups <= 0) return cudaSuccess;
+    k_pressure_groups<<<(n_groups + 255) / 256, 256, 0, s>>>(g, cf, tb, p, pn, vx, vy, vz, fx, fy, fz, solid,
+                                                             groups, n_groups);
     return cudaGetLastError();
 }
 

@@ -130,6 +130,11 @@ cudaError_t launch_velocity_general(const Grid& g, const Coef& cf, const Tables&
                                     const float* p, float* vx, float* vy, float* vz,
                                     const float* fx, const float* fy, const float* fz,
                                     cudaStream_t s, const unsigned* gate = nullptr);
+// pressure update of listed four-cell groups (plate-face neighbours after a walled single-pass step)
+cudaError_t launch_pressure_groups(const Grid& g, const Coef& cf, const Tables& tb, const float* p, float* pn,
+                                   const float* vx, const float* vy, const float* vz, const float* fx,
+                                   const float* fy, const float* fz, const uint8_t* solid,
+                                   const long long* groups, int n_groups, cudaStream_t s);
 cudaError_t launch_pressure_general(const Grid& g, const Coef& cf, const Tables& tb,
                                     const float* p, float* pn, const float* vx, const float* vy,
                                     const float* vz, const float* fx, const float* fy,
@@ -215,6 +220,12 @@ struct FusedArgs {
     const float* rec_w = nullptr;
     float* rec_out = nullptr;
     int n_rec = 0;
+    // Walled scenes (whole rooms only): open fractions of the Vx, Vy, Vz faces
+    // (null: none; a face with fraction 0 is closed), whether the divergence
+    // scales each face by its fraction, and the solid-cell mask (null: none).
+    const float* fr[3] = {nullptr, nullptr, nullptr};
+    bool frac_div = false;
+    const uint8_t* solid = nullptr;
 };
 struct FusedCache;         // host-side TMA descriptors of a handle's fields
 FusedCache* fused_cache_create();

@@ -85,14 +85,19 @@ def test_small_rooms_match_reference(torch_cuda, golden, kernel, tag, nx, ny, nz
         assert bits_equal(got.ravel(), arrays[f"{tag}/{k}"]), (k, first_mismatch(got, arrays[f"{tag}/{k}"]))
 
 
+@pytest.mark.parametrize("kernel", ["fused", "two_pass"])
 @pytest.mark.parametrize("tag,use_fracs,steps", [("body_fracs", True, 300), ("body_nofrac", False, 200)])
-def test_body_scene_matches_reference(torch_cuda, golden, tag, use_fracs, steps):
-    """Walls, plate with soundhole, bridge drive, plate force, cut-cell fractions."""
+def test_body_scene_matches_reference(torch_cuda, golden, tag, use_fracs, steps, kernel):
+    """Walls, plate with soundhole, bridge drive, plate force, cut-cell fractions,
+    on the two-pass kernels and on the walled single-pass step."""
     from spectral_analyzer_b200 import AcousticFDTD
     arrays, _ = golden
     sc = body_scene()
     f = AcousticFDTD(**sc.kwargs())
-    assert f.kernel == "two_pass"
+    assert f.kernel == "two_pass"          # the automatic choice for walled scenes
+    if kernel == "fused":
+        f.set_kernel("fused")
+    assert f.kernel == kernel
     out = drive_scene(f, sc, steps, use_fracs=use_fracs)
     for k, got in out.items():
         ref = arrays[f"{tag}/{k}"]
@@ -102,11 +107,13 @@ def test_body_scene_matches_reference(torch_cuda, golden, tag, use_fracs, steps)
             assert bits_equal(got, ref), (k, first_mismatch(got, ref))
 
 
-def test_reset_then_continue(torch_cuda, golden):
+@pytest.mark.parametrize("kernel", ["fused", "two_pass"])
+def test_reset_then_continue(torch_cuda, golden, kernel):
     from spectral_analyzer_b200 import AcousticFDTD
     arrays, meta = golden
     sc = body_scene(seed=1)
     f = AcousticFDTD(**sc.kwargs())
+    f.set_kernel(kernel)
     drive_scene(f, sc, 50)
     f.reset()
     out = drive_scene(f, sc, 30)
@@ -131,12 +138,14 @@ def test_pressure_instability_code(torch_cuda, golden, kernel):
         f.step(300)
 
 
-def test_plate_guard_code(torch_cuda, golden):
+@pytest.mark.parametrize("kernel", ["fused", "two_pass"])
+def test_plate_guard_code(torch_cuda, golden, kernel):
     from spectral_analyzer_b200 import AcousticFDTD
     _, meta = golden
     m = meta["unstable_plate"]
     sc = body_scene(seed=2)
     f = AcousticFDTD(**sc.kwargs())
+    f.set_kernel(kernel)
     f.set_bridge_sources(sc.bridge_idx, sc.bridge_wgt)
     rcs = []
     for _ in range(60):
@@ -301,3 +310,28 @@ def test_out_of_range_sampler_index_is_rejected(torch_cuda):
     idx = np.full(8, 12 ** 3, np.int32)
     with pytest.raises(ValueError):
         f.sample_pressure_precomputed(idx, np.ones(8, np.float32))
+
+
+@pytest.mark.parametrize("dims,use_fracs", [((170, 140, 74), True), ((61, 45, 37), False), ((40, 33, 140), True)])
+def test_walled_single_pass_equals_two_pass(torch_cuda, dims, use_fracs):
+    """Size-independent property on larger body scenes (guitar-body size
+    included): the walled single-pass step and the two-pass kernels agree bit
+    for bit on every sample and field after 150 driven steps."""
+    from spectral_analyzer_b200 import AcousticFDTD
+    sc = body_scene(*dims, seed=4, n_pml=6)
+    outs = []
+    for kernel in ("fused", "two_pass"):
+        f = AcousticFDTD(**sc.kwargs())
+        f.set_kernel(kernel)
+        out = drive_scene(f, sc, 150, use_fracs=use_fracs)
+        out["Vx"] = f.get_velocity_x().ravel()
+        out["Vy"] = f.get_velocity_y().ravel()
+        outs.append(out)
+        f.close()
+    assert np.any(outs[1]["P"] != 0)
+    for k in outs[1]:
+        a, b = np.asarray(outs[0][k]), np.asarray(outs[1][k])
+        if a.dtype == np.float32:
+            assert bits_equal(a, b), (k, first_mismatch(a, b))
+        else:
+            assert np.array_equal(a, b), k
