@@ -84,6 +84,10 @@ def parse_args():
     ap.add_argument("--scale-mode", choices=["split", "replicas"], default="split",
                     help="N>1: split the room into N slabs along i (strong scaling, one ghost exchange "
                          "per step overlapped with the interior) or run N independent replicas (weak)")
+    ap.add_argument("--walled", action="store_true",
+                    help="a walled body scene (solid cells, cut-cell fractions, Kirchhoff plate) on both step "
+                         "kernels; --grid sets its size (default 512,384,256)")
+    ap.add_argument("--walled-steps", type=int, default=200)
     ap.add_argument("--amr", action="store_true",
                     help="the AMR pressure backend on a box grid of --amr-cells^3 cells (gradient order 2, "
                          "anechoic border): cell-updates/s and bytes moved per cell-step")
@@ -761,6 +765,58 @@ def launch_ranks(n: int, argv) -> int:
         return 124
 
 
+def walled_arm(args):
+    """A body scene (back and rib walls, a plate with a soundhole, cut-cell face
+    fractions, bridge sources) stepped by the two-pass kernels and by the walled
+    single pass.  Per kernel: the step kernels' CUDA-event time per step (the
+    profile window: velocity + pressure, or the single pass + plate faces +
+    recomputed plate-face neighbours) and the wall time of fdtd_step(st, n),
+    which also runs the plate update and its guard read-back every step."""
+    import torch
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    sys.path.insert(0, os.path.join(ROOT, "tests", "golden"))
+    from scenes import body_scene
+    from spectral_analyzer_b200 import AcousticFDTD
+    dims = GRID or (512, 384, 256)
+    sc = body_scene(*dims, seed=4, n_pml=10)
+    cells = dims[0] * dims[1] * dims[2]
+    peak, peak_kind = measured_peak()
+    rows = {}
+    with ClockSampler(gpu_uuid(int(os.environ.get("LOCAL_RANK", "0")))) as clk:
+        for kernel in ("two_pass", "fused"):
+            f = AcousticFDTD(**sc.kwargs())
+            f.set_kernel(kernel)
+            f.set_face_fractions(*sc.fracs)
+            f.set_bridge_sources(sc.bridge_idx, sc.bridge_wgt)
+            f.step(10)
+            torch.cuda.synchronize()
+            f.profile(True)
+            t0 = time.perf_counter()
+            f.step(args.walled_steps)
+            torch.cuda.synchronize()
+            wall = (time.perf_counter() - t0) / args.walled_steps
+            ms, n, nk = f.profile_read()
+            kern_ms = ms / n
+            rows[kernel] = {"kernel_ms_per_step": kern_ms, "wall_ms_per_step": wall * 1e3,
+                            "gcell_updates_per_s_kernels": cells / kern_ms / 1e6,
+                            "gcell_updates_per_s_wall": cells / wall / 1e9, "launches": f.launch_count}
+            f.close()
+    bpu = 45   # P, Vx, Vy, Vz read and written (32 B), three face fractions (12 B), solid mask (1 B)
+    achieved = rows["fused"]["gcell_updates_per_s_kernels"] * bpu
+    line = {"metric": "Gcell-updates/s (walled scene, step kernels)", "value": rows["fused"]["gcell_updates_per_s_kernels"],
+            "unit": "Gcell-updates/s", "n_gpus": 1, "steps": args.walled_steps, "higher_is_better": True,
+            "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"body_scene{dims[0]}x{dims[1]}x{dims[2]}_walls_fractions_plate",
+                       "cells": cells, "plate_nodes": int(sc.kwargs()["plate_active"].sum())},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
+                         "kernel": "walled single pass (k_fused_step walls + plate faces + k_pressure_groups)",
+                         "algorithmic_bytes_per_update": bpu},
+            "kernels": rows, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def split_line(args, world, ms_max, e2e, launches, clocks, own_cells, cells, kind):
     """The JSON line of an N-rank split-room run (rank 0 prints it)."""
     step_ms = ms_max / args.steps
@@ -897,6 +953,8 @@ def main():
         return slab_arm(args)
     if args.amr:
         return amr_arm(args)
+    if args.walled:
+        return walled_arm(args)
     if world > 1 and args.scale_mode == "split":
         return split_arm(args)
     return engine_arm(args)

@@ -225,7 +225,7 @@ FDTD_B200_API int fdtd_b200_step_async(AcousticFDTDState* st, int n_steps);
 FDTD_B200_API int fdtd_b200_synchronize(AcousticFDTDState* st);
 
 /* Step-kernel selection: 0 automatic (fused single pass for open rooms and
- * for walled scenes of at least 2^24 cells, two-pass for smaller walled
+ * for walled scenes of at least 2^22 cells, two-pass for smaller walled
  * scenes), 1 two-pass, 2 fused.  Walled scenes (solid cells, face fractions,
  * an active plate) run the single pass with the walled rules; both kernels
  * give the same results bit for bit.  FDTD_ERR_ARG for 2 when the row

@@ -236,7 +236,7 @@ __device__ __forceinline__ void init_barriers(unsigned bar0)
 // walled-scene rules of the two-pass kernels to the general body: a face whose
 // open fraction is 0 is closed (its new velocity is 0), the divergence sees
 // each face's velocity times its fraction (when fractions were set), and
-// solid cells keep P = 0; the interior body is not used.
+// solid cells keep P = 0, in both the interior and the general body.
 template <class C, bool PEER = true, bool WALLS = false>
 __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap* tmP,
                                            const CUtensorMap* tmX, const CUtensorMap* tmY,
@@ -381,7 +381,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
     // evaluate the same expressions (alpha_x = 0, px = 1 there), so the results
     // do not depend on the choice.  The step runs in one wave, so a CTA left on
     // the general body for its whole march would set the kernel's time.
-    const bool clean = kfull && !WALLS;
+    const bool clean = kfull;
     int fast_lo = u1 + 1, fast_hi = u1 + 1;
     if (clean && a.tb.xi_hi > a.tb.xi_lo) {
         fast_lo = max(max(a.tb.xi_lo + 3, 3 - xg0), i_beg + 3);

@@ -312,7 +312,8 @@ def test_out_of_range_sampler_index_is_rejected(torch_cuda):
         f.sample_pressure_precomputed(idx, np.ones(8, np.float32))
 
 
-@pytest.mark.parametrize("dims,use_fracs", [((170, 140, 74), True), ((61, 45, 37), False), ((40, 33, 140), True)])
+@pytest.mark.parametrize("dims,use_fracs", [((170, 140, 74), True), ((61, 45, 37), False), ((40, 33, 140), True),
+                                            ((48, 40, 256), True)])
 def test_walled_single_pass_equals_two_pass(torch_cuda, dims, use_fracs):
     """Size-independent property on larger body scenes (guitar-body size
     included): the walled single-pass step and the two-pass kernels agree bit
