@@ -1,7 +1,7 @@
 // fdtd_tma.h — the PTX the TMA/mbarrier step kernels share: shared-memory
-// addresses, mbarriers with wall-time-bounded waits, 3-D tiled TMA loads (no
-// cluster multicast) and the tensor-map acquire; and the host encoder of a
-// tensor map over one padded field.
+// addresses, mbarriers with wall-time-bounded waits, plain 3-D tiled TMA
+// loads into the issuing CTA's own shared memory, and the tensor-map acquire;
+// and the host encoder of a tensor map over one padded field.
 #pragma once
 
 #include "fdtd_internal.h"
