@@ -554,7 +554,7 @@ __device__ __forceinline__ bool fused_tile(const FusedArgs& a, const CUtensorMap
                                     v = close4(v, fry);
                                 }
                             }
-                            if (r >= 2 && r < C::TJ + 2 && (FAST || kb < sz))
+                            if (r >= 2 && r < C::TJ + 2 && kb < sz)
                                 stg4(a.vout[1] + ib + (long long)jf * sz + kb, v);
                             if constexpr (WALLS) {
                                 if (a.fr[1] && a.frac_div && kb < sz) v = mul4(v, fry);
