@@ -468,7 +468,7 @@ bool fused_walled_ok(const AcousticFDTDState* st)
 
 // Walled scenes take the single pass automatically from this many cells on:
 // below it the fields stay in L2 and the two-pass kernels are faster (step
-// kernels per step, two-pass / single pass: 170x140x74 49 / 67 us,
+// kernels per step, two-pass / single pass: 170x140x74 40 / 67 us,
 // 160x128x128 50 / 60; above it 256x200x128 120 / 106, 400x300x256 511 / 430,
 // 512x384x256 827 / 558).
 constexpr long long kWalledFusedCells = 1LL << 22;

@@ -30,12 +30,17 @@ __device__ __forceinline__ void st4(float* p, long long i, const float (&v)[4])
 __device__ __forceinline__ void unpack(const float4& x, float (&v)[4]) { v[0] = x.x; v[1] = x.y; v[2] = x.z; v[3] = x.w; }
 
 // Threads own four consecutive cells k0 .. k0+3 of a row (k0 a multiple of 4;
-// rows start on 8-float boundaries, so every float4 access is aligned).
+// rows start on 8-float boundaries, so every float4 access is aligned).  The
+// (row, group) pairs of a plane are numbered consecutively over 1-D blocks,
+// so no lane idles when Nz/4 is not a multiple of the warp width (Nz = 74:
+// 19 groups per row), and consecutive lanes read consecutive 16-byte groups.
 #define GEN_INDEX                                                          \
-    const int k0 = 4 * (blockIdx.x * blockDim.x + threadIdx.x);            \
-    const int j = blockIdx.y * blockDim.y + threadIdx.y;                   \
-    const int i = blockIdx.z;                                              \
-    if (k0 >= g.nz || j >= g.ny) return;                                   \
+    const int nq_ = (g.nz + 3) >> 2;                                       \
+    const int t_ = blockIdx.x * blockDim.x + threadIdx.x;                  \
+    if (t_ >= g.ny * nq_) return;                                          \
+    const int j = t_ / nq_;                                                \
+    const int k0 = 4 * (t_ - j * nq_);                                     \
+    const int i = blockIdx.y;                                              \
     const long long id = ((long long)i * g.ny + j) * g.sz + k0;
 
 // Velocity update on the three staggered face sets (acoustic_fdtd.cpp:1099-1148),
@@ -347,8 +352,8 @@ cudaError_t launch_velocity_general(const Grid& g, const Coef& cf, const Tables&
                                     const float* fx, const float* fy, const float* fz,
                                     cudaStream_t s, const unsigned* gate)
 {
-    dim3 block(32, 8, 1);
-    dim3 grid((g.sz / 4 + 31) / 32, (g.ny + 7) / 8, g.nx);
+    dim3 block(256, 1, 1);
+    dim3 grid((g.ny * ((g.nz + 3) / 4) + 255) / 256, g.nx, 1);
     k_velocity_general<<<grid, block, 0, s>>>(g, cf, tb, p, vx, vy, vz, fx, fy, fz, gate);
     return cudaGetLastError();
 }
@@ -359,8 +364,8 @@ cudaError_t launch_pressure_general(const Grid& g, const Coef& cf, const Tables&
                                     const float* fz, const uint8_t* solid, cudaStream_t s,
                                     const unsigned* gate)
 {
-    dim3 block(32, 8, 1);
-    dim3 grid((g.sz / 4 + 31) / 32, (g.ny + 7) / 8, g.nx);
+    dim3 block(256, 1, 1);
+    dim3 grid((g.ny * ((g.nz + 3) / 4) + 255) / 256, g.nx, 1);
     k_pressure_general<<<grid, block, 0, s>>>(g, cf, tb, p, pn, vx, vy, vz, fx, fy, fz, solid, gate);
     return cudaGetLastError();
 }
