@@ -15,14 +15,17 @@
  *
  * Reverse step n, given Lp = dL/dp~^{n+1} and Lv = dL/dv^{n+1/2} (partial,
  * through step n+1's velocity update) and r^n = dL/dy^n:
- *   lam  = Lp + R^T r^n                        (k_inject)
+ *   lam  = Lp + R^T r^n                        (inside k_adj_cells1)
  *   U    = lam (.) q ;  g_c -= q_c^2 lam_c z_c, z = p~^n - bulk D v^{n+1/2}   (k_adj_cells1)
  *   mu   = Lv - bulk D^T U ;  W = mu (.) d ;  E_f = mu_f y_f,
  *          y = v^{n-1/2} - vc G p~^n ;  Lv <- W                            (k_adj_faces)
  *   Lp  <- U - vc G^T W ;  g_c -= 1/2 sum_{faces f of c} E_f               (k_adj_cells2)
  * Gradients accumulate in double.  The forward is recomputed segment by
- * segment from checkpoints (p^n and v^{n-1/2} every K steps) into K+1
+ * segment from checkpoints (p~^n and v^{n-1/2} every K steps) into K+1
  * device slots, so the reverse sweep reads every state it needs from HBM.
+ * Launches per step: forward 3 (velocity, pressure, an epilogue that records
+ * the receivers and then adds the next step's source sample), recompute 2
+ * (the pressure kernel adds the next sample), reverse 3.
  * Each sweep (forward, forward with checkpoints, backward) is captured once
  * as a CUDA graph and replayed while its length and buffers stay the same:
  * a gradient evaluation is then two graph launches.
@@ -271,11 +274,14 @@ __global__ void __launch_bounds__(256) k_fwd_vel(Grid g, ACoef<R> cf, const R* _
     }
 }
 
+// dep >= 0: the next step's source sample sig[dep_n] is added to the new
+// pressure of cell dep, as k_deposit would before that step.
 template <class R>
 __global__ void __launch_bounds__(256) k_fwd_pres(Grid g, ACoef<R> cf, const R* __restrict__ a,
                                                   const R* __restrict__ p, const R* __restrict__ vx,
                                                   const R* __restrict__ vy, const R* __restrict__ vz,
-                                                  R* __restrict__ pn)
+                                                  R* __restrict__ pn, long long dep, const R* __restrict__ sig,
+                                                  int dep_n)
 {
     ADJ4_INDEX
     R dv[4], pc[4], ac[4], out[4];
@@ -285,6 +291,12 @@ __global__ void __launch_bounds__(256) k_fwd_pres(Grid g, ACoef<R> cf, const R* 
 #pragma unroll
     for (int q = 0; q < 4; ++q)
         out[q] = (k0 + q < g.nz) ? rmul(rsub(pc[q], rmul(cf.bulk, dv[q])), cell_q(ac[q])) : R(0);
+    if (dep >= id && dep < id + 4) {
+        const R sv = sig[dep_n];
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+            if (dep == id + q && sv != R(0)) out[q] = radd(out[q], sv);
+    }
     st4r(pn, id, out);
 }
 
@@ -296,40 +308,70 @@ __global__ void k_deposit(R* p, long long src, const R* sig, int n)
     if (s != R(0)) p[src] = radd(p[src], s);
 }
 
-// Receivers after step n, summed as w0*p0 + w1*p1 + ... (acoustic_fdtd.cpp:1663-1676).
+// After forward step n: the receivers of P^{n+1} (row; 8 taps summed
+// w0*p0 + w1*p1 + ... as acoustic_fdtd.cpp:1663-1676), then the next step's
+// source sample into P^{n+1} (dep_n >= 0); one block.
 template <class R>
-__global__ void k_record(const R* p, int n_rec, const long long* idx, const R* w, R* row)
+__global__ void k_fwd_epilogue(R* p, int n_rec, const long long* idx, const R* w, R* row, long long src,
+                               const R* sig, int dep_n)
 {
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= n_rec) return;
-    R s = rmul(w[8 * r], p[idx[8 * r]]);
-    for (int t = 1; t < 8; ++t) s = radd(s, rmul(w[8 * r + t], p[idx[8 * r + t]]));
-    row[r] = s;
-}
-
-// lam = Lp + R^T r^n: one thread, so taps that share a cell add in order.
-template <class R>
-__global__ void k_inject(R* lp, int n_rec, const long long* idx, const R* w, const R* rrow)
-{
-    for (int r = 0; r < n_rec; ++r)
-        for (int t = 0; t < 8; ++t) lp[idx[8 * r + t]] = radd(lp[idx[8 * r + t]], rmul(w[8 * r + t], rrow[r]));
+    if (row)
+        for (int r = threadIdx.x; r < n_rec; r += blockDim.x) {
+            R s = rmul(w[8 * r], p[idx[8 * r]]);
+            for (int t = 1; t < 8; ++t) s = radd(s, rmul(w[8 * r + t], p[idx[8 * r + t]]));
+            row[r] = s;
+        }
+    __syncthreads();
+    if (threadIdx.x == 0 && dep_n >= 0 && src >= 0) {
+        const R sv = sig[dep_n];
+        if (sv != R(0)) p[src] = radd(p[src], sv);
+    }
 }
 
 __device__ __forceinline__ void ld4d(const double* p, long long i, double (&v)[4]) { ld4r<double>(p, i, v); }
 __device__ __forceinline__ void st4d(double* p, long long i, const double (&v)[4]) { st4r<double>(p, i, v); }
+
+// The receivers' adjoint sources, by cell: the distinct tap cells in
+// ascending order, and for each its taps (8 r + t) in the order R^T adds them.
+template <class R>
+struct TapSources {
+    int n = 0;                       // distinct tap cells (0: none)
+    const long long* cell = nullptr;
+    const int* start = nullptr;      // [n + 1]
+    const int* tap = nullptr;        // 8 r + t, ascending within a cell
+    const R* w = nullptr;            // tap weights [8 n_rec]
+    const R* rrow = nullptr;         // this step's receiver residuals [n_rec]
+};
 
 template <class R>
 __global__ void __launch_bounds__(256) k_adj_cells1(Grid g, ACoef<R> cf, const R* __restrict__ a,
                                                     const R* __restrict__ lam, const R* __restrict__ pt,
                                                     const R* __restrict__ vx, const R* __restrict__ vy,
                                                     const R* __restrict__ vz, R* __restrict__ u,
-                                                    double* __restrict__ grad)
+                                                    double* __restrict__ grad, TapSources<R> ts)
 {
     ADJ4_INDEX
     R ac[4], l[4], ptc[4], dv[4], uo[4];
     double gr[4];
     ld4r(a, id, ac);
     ld4r(lam, id, l);
+    if (ts.n > 0) {   // lam = Lp + R^T r^n on the tap cells among these four
+        int lo = 0, hi = ts.n;   // first tap cell >= id
+        while (lo < hi) {
+            const int mid = (lo + hi) >> 1;
+            if (ts.cell[mid] < id) lo = mid + 1;
+            else hi = mid;
+        }
+        for (int c = lo; c < ts.n && ts.cell[c] < id + 4; ++c) {
+            const int q = (int)(ts.cell[c] - id);
+            for (int e = ts.start[c]; e < ts.start[c + 1]; ++e) {
+                const int tp = ts.tap[e];
+#pragma unroll
+                for (int qq = 0; qq < 4; ++qq)
+                    if (qq == q) l[qq] = radd(l[qq], rmul(ts.w[tp], ts.rrow[tp >> 3]));
+            }
+        }
+    }
     ld4r(pt, id, ptc);
     div4(g, vx, vy, vz, id, i, j, k0, cf, dv);
     ld4d(grad, id, gr);
@@ -569,6 +611,10 @@ struct FdtdB200Adj {
     void* rw = nullptr;            // R[8 n_rec]
     void* traces = nullptr;        // R[n_steps x n_rec]
     void* resid = nullptr;         // R[n_steps x n_rec]
+    int n_tap_cells = 0;           // distinct receiver tap cells, sorted (TapSources)
+    long long* tap_cell = nullptr;
+    int* tap_start = nullptr;
+    int* tap_ord = nullptr;
     int trace_cap = 0;
     int fwd_steps = -1;            // steps of the last checkpointed forward
     std::vector<void*> allocs;
@@ -615,25 +661,30 @@ const ACoef<float>& coef<float>(const FdtdB200Adj* h) { return h->c32; }
 template <>
 const ACoef<double>& coef<double>(const FdtdB200Adj* h) { return h->c64; }
 
-// One forward step from (p, vin) to (pn, vout); p is first given the source.
+// One forward step from (p, vin) to (pn, vout); p already holds this step's
+// source sample.  With next_deposit the next step's sample is added to pn:
+// by the pressure kernel when no receivers are recorded (a recompute), else
+// by the epilogue after it has recorded the receivers of pn.
 template <class R>
-void fwd_step(FdtdB200Adj* h, int n, void* p, void* const* vin, void* const* vout, void* pn)
+void fwd_step(FdtdB200Adj* h, int n, void* p, void* const* vin, void* const* vout, void* pn, bool next_deposit,
+              bool record)
 {
     const Grid& g = h->g;
     const ACoef<R>& cf = coef<R>(h);
-    if (h->src >= 0 && n < h->n_sig) {
-        k_deposit<R><<<1, 1, 0, h->stream>>>((R*)p, h->src, (const R*)h->sig, n);
-        ++h->launches;
-    }
+    const bool dep = next_deposit && h->src >= 0 && n + 1 < h->n_sig;
+    const bool rec = record && h->n_rec > 0 && n < h->trace_cap;
     k_fwd_vel<R><<<vec_grid(g), kBlock, 0, h->stream>>>(g, cf, (const R*)h->a, (const R*)p, (const R*)vin[0],
                                                          (const R*)vin[1], (const R*)vin[2], (R*)vout[0],
                                                          (R*)vout[1], (R*)vout[2]);
+    const bool dep_in_pres = dep && !rec;
     k_fwd_pres<R><<<vec_grid(g), kBlock, 0, h->stream>>>(g, cf, (const R*)h->a, (const R*)p, (const R*)vout[0],
-                                                          (const R*)vout[1], (const R*)vout[2], (R*)pn);
+                                                          (const R*)vout[1], (const R*)vout[2], (R*)pn,
+                                                          dep_in_pres ? h->src : -1LL, (const R*)h->sig, n + 1);
     h->launches += 2;
-    if (h->n_rec > 0 && n < h->trace_cap) {
-        k_record<R><<<(h->n_rec + 31) / 32, 32, 0, h->stream>>>((const R*)pn, h->n_rec, h->ridx, (const R*)h->rw,
-                                                               (R*)h->traces + (size_t)n * h->n_rec);
+    if (rec) {
+        k_fwd_epilogue<R><<<1, 128, 0, h->stream>>>((R*)pn, h->n_rec, h->ridx, (const R*)h->rw,
+                                                    (R*)h->traces + (size_t)n * h->n_rec, h->src,
+                                                    (const R*)h->sig, dep ? n + 1 : -1);
         ++h->launches;
     }
 }
@@ -667,14 +718,18 @@ int forward_impl(FdtdB200Adj* h, int n_steps, int keep)
     void* P[2] = {h->P0, h->P1};
     void* V[2][3] = {{h->V0[0], h->V0[1], h->V0[2]}, {h->V1[0], h->V1[1], h->V1[2]}};
     int cur = 0;
+    if (h->src >= 0 && h->n_sig > 0) {   // step 0's source sample; later ones come with the step before
+        k_deposit<R><<<1, 1, 0, h->stream>>>((R*)P[cur], h->src, (const R*)h->sig, 0);
+        ++h->launches;
+    }
     for (int n = 0; n < n_steps; ++n) {
-        if (keep && n % h->K == 0) {
+        if (keep && n % h->K == 0) {   // p~^n: P^n with its source sample
             const int q = n / h->K;
             ACK(cudaMemcpyAsync(h->ckP[q], P[cur], fb, cudaMemcpyDeviceToDevice, h->stream));
             for (int c = 0; c < 3; ++c)
                 ACK(cudaMemcpyAsync(h->ckV[3 * q + c], V[cur][c], fb, cudaMemcpyDeviceToDevice, h->stream));
         }
-        fwd_step<R>(h, n, P[cur], V[cur], V[cur ^ 1], P[cur ^ 1]);
+        fwd_step<R>(h, n, P[cur], V[cur], V[cur ^ 1], P[cur ^ 1], n + 1 < n_steps, true);
         cur ^= 1;
     }
     ACK(cudaGetLastError());
@@ -777,24 +832,27 @@ int backward_impl(FdtdB200Adj* h)
         ACK(cudaMemcpyAsync(h->sP[0], h->ckP[s], fb, cudaMemcpyDeviceToDevice, h->stream));
         for (int c = 0; c < 3; ++c)
             ACK(cudaMemcpyAsync(h->sV[c], h->ckV[3 * s + c], fb, cudaMemcpyDeviceToDevice, h->stream));
-        // recompute: slot t holds p~^{n0+t} (after its deposit) and v^{n0+t-1/2}
-        const int saved_cap = h->trace_cap;
-        h->trace_cap = 0;   // traces are already recorded
+        // recompute: slot t holds p~^{n0+t} (after its deposit; the checkpoint
+        // already holds it) and v^{n0+t-1/2}; traces are already recorded
         for (int t = 0; t < len; ++t)
-            fwd_step<R>(h, n0 + t, h->sP[t], &h->sV[3 * t], &h->sV[3 * (t + 1)], h->sP[t + 1]);
-        h->trace_cap = saved_cap;
+            fwd_step<R>(h, n0 + t, h->sP[t], &h->sV[3 * t], &h->sV[3 * (t + 1)], h->sP[t + 1], t + 1 < len,
+                        false);
         for (int t = len - 1; t >= 0; --t) {
             const int n = n0 + t;
             void* const* vo = &h->sV[3 * t];       // v^{n-1/2}
             void* const* vn = &h->sV[3 * (t + 1)]; // v^{n+1/2}
+            TapSources<R> ts;   // R^T r^n, added to Lp inside k_adj_cells1
             if (h->n_rec > 0) {
-                k_inject<R><<<1, 1, 0, h->stream>>>((R*)h->Lp, h->n_rec, h->ridx, (const R*)h->rw,
-                                                    (const R*)h->resid + (size_t)n * h->n_rec);
-                ++h->launches;
+                ts.n = h->n_tap_cells;
+                ts.cell = h->tap_cell;
+                ts.start = h->tap_start;
+                ts.tap = h->tap_ord;
+                ts.w = (const R*)h->rw;
+                ts.rrow = (const R*)h->resid + (size_t)n * h->n_rec;
             }
             k_adj_cells1<R><<<vec_grid(g), kBlock, 0, h->stream>>>(
                 g, cf, (const R*)h->a, (const R*)h->Lp, (const R*)h->sP[t], (const R*)vn[0], (const R*)vn[1],
-                (const R*)vn[2], (R*)h->U, h->grad);
+                (const R*)vn[2], (R*)h->U, h->grad, ts);
             k_adj_faces<R><<<vec_grid(g), kBlock, 0, h->stream>>>(
                 g, cf, (const R*)h->a, (const R*)h->U, (const R*)h->sP[t], (const R*)vo[0], (const R*)vo[1],
                 (const R*)vo[2], (R*)h->Lv[0], (R*)h->Lv[1], (R*)h->Lv[2], (R*)h->E[0], (R*)h->E[1],
@@ -960,6 +1018,18 @@ int fdtd_b200_adj_set_receivers(FdtdB200Adj* h, int n_rec, const int* idx8, cons
     dfree(h, h->rw);
     dfree(h, h->traces);
     dfree(h, h->resid);
+    {
+        void* t1 = h->tap_cell;
+        void* t2 = h->tap_start;
+        void* t3 = h->tap_ord;
+        dfree(h, t1);
+        dfree(h, t2);
+        dfree(h, t3);
+    }
+    h->tap_cell = nullptr;
+    h->tap_start = nullptr;
+    h->tap_ord = nullptr;
+    h->n_tap_cells = 0;
     h->n_rec = n_rec;
     h->trace_cap = max_steps;
     if (n_rec > 0) {
@@ -978,6 +1048,35 @@ int fdtd_b200_adj_set_receivers(FdtdB200Adj* h, int n_rec, const int* idx8, cons
         }
         ACK(cudaMemcpyAsync(h->ridx, pi.data(), pi.size() * sizeof(long long), cudaMemcpyHostToDevice, h->stream));
         ACK(cudaMemcpyAsync(h->rw, wb.data(), wb.size(), cudaMemcpyHostToDevice, h->stream));
+        // taps grouped by cell, each cell's taps in ascending 8 r + t (the order
+        // in which R^T r adds them one after another)
+        std::vector<int> ord(pi.size());
+        for (size_t q = 0; q < ord.size(); ++q) ord[q] = (int)q;
+        std::stable_sort(ord.begin(), ord.end(), [&](int x, int y) { return pi[x] < pi[y]; });
+        std::vector<long long> cells;
+        std::vector<int> start;
+        for (size_t e = 0; e < ord.size(); ++e)
+            if (e == 0 || pi[ord[e]] != pi[ord[e - 1]]) {
+                cells.push_back(pi[ord[e]]);
+                start.push_back((int)e);
+            }
+        start.push_back((int)ord.size());
+        void* tc = nullptr;
+        void* tsb = nullptr;
+        void* to = nullptr;
+        rc = dalloc(h, &tc, cells.size() * sizeof(long long));
+        if (!rc) rc = dalloc(h, &tsb, start.size() * sizeof(int));
+        if (!rc) rc = dalloc(h, &to, ord.size() * sizeof(int));
+        if (rc) return rc;
+        h->tap_cell = (long long*)tc;
+        h->tap_start = (int*)tsb;
+        h->tap_ord = (int*)to;
+        h->n_tap_cells = (int)cells.size();
+        ACK(cudaMemcpyAsync(h->tap_cell, cells.data(), cells.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                            h->stream));
+        ACK(cudaMemcpyAsync(h->tap_start, start.data(), start.size() * sizeof(int), cudaMemcpyHostToDevice,
+                            h->stream));
+        ACK(cudaMemcpyAsync(h->tap_ord, ord.data(), ord.size() * sizeof(int), cudaMemcpyHostToDevice, h->stream));
         ACK(cudaStreamSynchronize(h->stream));
     }
     h->fwd_steps = -1;
