@@ -168,6 +168,10 @@ struct AcousticFDTDState {
     long long* h_sidx = nullptr;
     float* h_sw = nullptr;
     float* h_sout = nullptr;
+    // sampler results written by the kernel straight into pinned host memory
+    // (mapped into the device's address space): no device-to-host copy per call
+    float* h_sout_map = nullptr;
+    float* d_sout_map = nullptr;
     // what d_sidx / d_sw hold (upload_taps skips a copy of the same taps)
     std::vector<long long> up_idx;
     std::vector<float> up_w;
@@ -313,9 +317,10 @@ int ensure_scratch(AcousticFDTDState* st, size_t n)
     if (n <= st->s_cap) return FDTD_OK;
     size_t cap = std::max<size_t>(n, 1024);
     cudaFree(st->d_sidx); cudaFree(st->d_sw); cudaFree(st->d_sout);
-    cudaFreeHost(st->h_sidx); cudaFreeHost(st->h_sw); cudaFreeHost(st->h_sout);
+    cudaFreeHost(st->h_sidx); cudaFreeHost(st->h_sw); cudaFreeHost(st->h_sout); cudaFreeHost(st->h_sout_map);
     st->d_sidx = nullptr; st->d_sw = st->d_sout = nullptr;
     st->h_sidx = nullptr; st->h_sw = st->h_sout = nullptr;
+    st->h_sout_map = st->d_sout_map = nullptr;
     st->s_cap = 0;
     st->up_idx.clear();
     st->up_w.clear();
@@ -325,6 +330,8 @@ int ensure_scratch(AcousticFDTDState* st, size_t n)
     CK(cudaMallocHost(&st->h_sidx, cap * sizeof(long long)));
     CK(cudaMallocHost(&st->h_sw, cap * sizeof(float)));
     CK(cudaMallocHost(&st->h_sout, cap * sizeof(float)));
+    CK(cudaHostAlloc(&st->h_sout_map, cap * sizeof(float), cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer((void**)&st->d_sout_map, st->h_sout_map, 0));
     st->s_cap = cap;
     return FDTD_OK;
 }
@@ -354,12 +361,10 @@ int run_wsum(AcousticFDTDState* st, const float* field, int n_out, int taps, int
     if (n_out <= 0) return FDTD_OK;
     const size_t n = (size_t)n_out * taps;
     if (int rc = upload_taps(st, n, st->stream)) return rc;
-    CK(launch_wsum(field, st->d_sidx, st->d_sw, n_out, taps, from_zero, st->d_sout, st->stream));
+    CK(launch_wsum(field, st->d_sidx, st->d_sw, n_out, taps, from_zero, st->d_sout_map, st->stream));
     ++st->launches;
-    CK(cudaMemcpyAsync(st->h_sout, st->d_sout, (size_t)n_out * sizeof(float), cudaMemcpyDeviceToHost,
-                       st->stream));
     CK(cudaStreamSynchronize(st->stream));
-    memcpy(out, st->h_sout, (size_t)n_out * sizeof(float));
+    memcpy(out, st->h_sout_map, (size_t)n_out * sizeof(float));
     return FDTD_OK;
 }
 
@@ -748,7 +753,7 @@ void free_state(AcousticFDTDState* st)
     cudaFree(st->d_rec_idx); cudaFree(st->d_rec_w); cudaFree(st->d_trace);
     cudaFree(st->d_status); cudaFreeHost(st->h_status);
     cudaFree(st->d_sidx); cudaFree(st->d_sw); cudaFree(st->d_sout);
-    cudaFreeHost(st->h_sidx); cudaFreeHost(st->h_sw); cudaFreeHost(st->h_sout);
+    cudaFreeHost(st->h_sidx); cudaFreeHost(st->h_sw); cudaFreeHost(st->h_sout); cudaFreeHost(st->h_sout_map);
     for (cudaEvent_t e : st->prof.ev) cudaEventDestroy(e);
     fused_cache_destroy(st->fcache);
     if (st->own_stream) cudaStreamDestroy(st->own_stream);
