@@ -73,6 +73,30 @@ struct ProfEvents {
 
 }  // namespace
 
+// Everything a co-evolver substep's device work depends on besides memory
+// contents: buffer pointers, coefficients, flags.  A substep whose key equals a
+// cached one replays that graph (compared byte for byte; zero-filled first).
+struct SubstepKey {
+    cudaStream_t stream;
+    const float *p, *pn, *v0, *v1, *v2, *w_cur, *w_prev, *w_tmp, *frac[3], *ext, *h_ext;
+    const uint8_t* solid;
+    const long long *sidx;
+    const float *sw;
+    float *sout, *h_sout;
+    unsigned *status, *h_status;
+    Grid g;
+    Coef cf;
+    Tables tb;
+    PlateCoef pc;
+    int n_act, n_plate, n_saddle, ext_copy, ext_zero, has_frac;
+};
+
+struct SubstepGraph {
+    SubstepKey key;
+    cudaGraphExec_t exec = nullptr;
+    long long launches = 0;
+};
+
 struct AcousticFDTDState {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -83,6 +107,7 @@ struct AcousticFDTDState {
     float dx = 0, c = 0, rho = 0, dt = 0;
     Coef cf{};
     PlateCoef pc{};
+    std::vector<SubstepGraph> sgraphs;   // cached substep graphs (at most kSubstepGraphs)
     float a6[6] = {1, 1, 1, 1, 1, 1};
 
     float* p[2] = {nullptr, nullptr};
@@ -738,6 +763,9 @@ void free_state(AcousticFDTDState* st)
     cudaGetDevice(&d);
     if (d != st->device) cudaSetDevice(st->device);
     if (st->stream) cudaStreamSynchronize(st->stream);
+    for (auto& sg : st->sgraphs)
+        if (sg.exec) cudaGraphExecDestroy(sg.exec);
+    st->sgraphs.clear();
     if (st->own_fields) {
         cudaFree(st->p[0]); cudaFree(st->p[1]);
         for (int b = 0; b < 2; ++b)
@@ -1954,6 +1982,8 @@ long long fdtd_b200_batch_launch_count(const FdtdB200Batch* b) { return b ? b->l
 // handle exactly as fdtd_step leaves it on that failure.
 namespace {
 
+constexpr size_t kSubstepGraphs = 12;   // 2 pressure parities x 3 plate rotations, with / without forces
+
 int substep_plate(AcousticFDTDState* st, int n_saddle, float* out)
 {
     cudaStream_t s = st->stream;
@@ -1963,59 +1993,112 @@ int substep_plate(AcousticFDTDState* st, int n_saddle, float* out)
         st->ps_done_step = st->step_count;
     }
     const bool ext_was_pending = st->ext_pending;
-    if (st->ext_pending) {
-        CK(cudaMemcpyAsync(st->d_ext, st->h_ext, (size_t)st->N_plate * sizeof(float), cudaMemcpyHostToDevice, s));
-        st->dev_ext_nonzero = true;
-    }
-    const unsigned* gate = st->d_status;
-    CK(cudaMemsetAsync(st->d_status + kStatusPlate, 0xFF, sizeof(unsigned), s));
-    CK(launch_plate_step(st->n_act, st->d_act, st->d_nb13, st->d_above, st->d_below, st->d_w[st->wi_cur],
-                         st->d_w[st->wi_prev], st->d_w[st->wi_tmp], st->d_ext, st->P(), st->pc, st->d_status, s));
-    ++st->launches;
-    if (st->dev_ext_nonzero) {
-        CK(launch_zero_gated(st->d_ext, st->N_plate, gate, s));
-        ++st->launches;
-    }
-    // the rest of the step as if the plate update succeeded
+    if (st->ext_pending) st->dev_ext_nonzero = true;
+    const bool ext_zero = st->dev_ext_nonzero;
+    if (n_saddle > 0)   // the saddle taps (staged by the caller) go up before the step's work
+        if (int rc2 = upload_taps(st, (size_t)n_saddle * 4, s)) return rc2;
     const int wp0 = st->wi_prev, wc0 = st->wi_cur, wt0 = st->wi_tmp;
+    const bool record = st->n_rec > 0 && st->trace_len < st->trace_cap;
+    const int step1 = st->step_count + 1;
+    const bool checked = (step1 & (kCheckPeriod - 1)) == 0;
+    const int phase0 = st->stab_phase;
+    const int trace0 = st->trace_len;
+    const unsigned* gate = st->d_status;
+    float* const P = st->P();
+    float* const Pn = st->Pn();
+    const bool hf = st->has_frac;
+    // The substep's device work in stream order: the plate update (its guard
+    // gates everything after it), the step as if the plate succeeded (the
+    // plate's new displacement is d_w[wt0], the previous one d_w[wc0]), then
+    // the saddle samples and the status words to the host.
+    auto issue = [&]() -> int {
+        if (ext_was_pending)
+            CK(cudaMemcpyAsync(st->d_ext, st->h_ext, (size_t)st->N_plate * sizeof(float), cudaMemcpyHostToDevice, s));
+        CK(cudaMemsetAsync(st->d_status + kStatusPlate, 0xFF, sizeof(unsigned), s));
+        CK(launch_plate_step(st->n_act, st->d_act, st->d_nb13, st->d_above, st->d_below, st->d_w[wc0], st->d_w[wp0],
+                             st->d_w[wt0], st->d_ext, P, st->pc, st->d_status, s));
+        if (ext_zero) CK(launch_zero_gated(st->d_ext, st->N_plate, gate, s));
+        CK(launch_velocity_general(st->g, st->cf, st->tb, P, st->V(0), st->V(1), st->V(2), st->d_frac[0],
+                                   st->d_frac[1], st->d_frac[2], s, gate));
+        CK(launch_plate_inject(st->n_act, st->d_act, st->d_vzb, st->d_vza, st->d_w[wt0], st->d_w[wc0], st->cf.inv_dt,
+                               st->V(2), s, gate));
+        CK(launch_pressure_general(st->g, st->cf, st->tb, P, Pn, st->V(0), st->V(1), st->V(2),
+                                   hf ? st->d_frac[0] : nullptr, hf ? st->d_frac[1] : nullptr,
+                                   hf ? st->d_frac[2] : nullptr, st->d_solid, s, gate));
+        if (record)
+            CK(launch_wsum(Pn, st->d_rec_idx, st->d_rec_w, st->n_rec, 8, 0,
+                           st->d_trace + (size_t)trace0 * st->n_rec, s));
+        if (checked) {
+            CK(cudaMemsetAsync(st->d_status + kStatusCell, 0xFF, sizeof(unsigned), s));
+            CK(launch_check(st->g, Pn, st->N, phase0, st->d_status, step1, s, gate));
+        }
+        if (n_saddle > 0) {
+            CK(launch_wsum(st->d_w[wt0], st->d_sidx, st->d_sw, n_saddle, 4, 0, st->d_sout, s));
+            CK(cudaMemcpyAsync(st->h_sout, st->d_sout, (size_t)n_saddle * sizeof(float), cudaMemcpyDeviceToHost, s));
+        }
+        CK(cudaMemcpyAsync(st->h_status, st->d_status, kStatusWords * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+        return FDTD_OK;
+    };
+    const long long n_launch = 4 + (ext_zero ? 1 : 0) + (record ? 1 : 0) + (checked ? 1 : 0) + (n_saddle > 0 ? 1 : 0);
+    bool issued = false;
+    if (!record && !checked) {
+        // The same work recurs every substep with one of a few pointer sets:
+        // replay it as a cached CUDA graph (one launch instead of about ten).
+        SubstepKey k;
+        memset(&k, 0, sizeof k);
+        k.stream = s;
+        k.p = P; k.pn = Pn; k.v0 = st->V(0); k.v1 = st->V(1); k.v2 = st->V(2);
+        k.w_cur = st->d_w[wc0]; k.w_prev = st->d_w[wp0]; k.w_tmp = st->d_w[wt0];
+        for (int c2 = 0; c2 < 3; ++c2) k.frac[c2] = st->d_frac[c2];
+        k.ext = st->d_ext; k.h_ext = st->h_ext; k.solid = st->d_solid;
+        k.sidx = st->d_sidx; k.sw = st->d_sw; k.sout = st->d_sout; k.h_sout = st->h_sout;
+        k.status = st->d_status; k.h_status = st->h_status;
+        k.g = st->g; k.cf = st->cf; k.tb = st->tb; k.pc = st->pc;
+        k.n_act = st->n_act; k.n_plate = st->N_plate; k.n_saddle = n_saddle;
+        k.ext_copy = ext_was_pending; k.ext_zero = ext_zero; k.has_frac = hf;
+        SubstepGraph* hit = nullptr;
+        for (auto& sg : st->sgraphs)
+            if (memcmp(&sg.key, &k, sizeof k) == 0) hit = &sg;
+        const cudaError_t e_begin = hit ? cudaSuccess : cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e_begin != cudaSuccess) cudaGetLastError();   // e.g. the legacy default stream: no capture
+        if (!hit && e_begin == cudaSuccess) {
+            const int rc_issue = issue();
+            cudaGraph_t graph = nullptr;
+            const cudaError_t e_end = cudaStreamEndCapture(s, &graph);
+            cudaGraphExec_t exec = nullptr;
+            const cudaError_t e_inst = (rc_issue == FDTD_OK && e_end == cudaSuccess)
+                                           ? cudaGraphInstantiate(&exec, graph, 0) : cudaErrorUnknown;
+            if (graph) cudaGraphDestroy(graph);
+            cudaGetLastError();   // a capture that failed leaves its error behind; the direct path follows
+            if (e_inst == cudaSuccess) {
+                if (st->sgraphs.size() >= kSubstepGraphs) {
+                    cudaGraphExecDestroy(st->sgraphs.front().exec);
+                    st->sgraphs.erase(st->sgraphs.begin());
+                }
+                SubstepGraph sg;
+                sg.key = k;
+                sg.exec = exec;
+                sg.launches = n_launch;
+                st->sgraphs.push_back(sg);
+                hit = &st->sgraphs.back();
+            }
+        }
+        if (hit) {
+            CK(cudaGraphLaunch(hit->exec, s));
+            issued = true;
+        }
+    }
+    if (!issued)
+        if (int rc_issue = issue()) return rc_issue;
+    st->launches += n_launch;
+    // the bookkeeping of a step whose plate update succeeded (undone below if not)
     st->wi_prev = wc0;
     st->wi_cur = wt0;
     st->wi_tmp = wp0;
-    CK(launch_velocity_general(st->g, st->cf, st->tb, st->P(), st->V(0), st->V(1), st->V(2), st->d_frac[0],
-                               st->d_frac[1], st->d_frac[2], s, gate));
-    CK(launch_plate_inject(st->n_act, st->d_act, st->d_vzb, st->d_vza, st->d_w[st->wi_cur], st->d_w[st->wi_prev],
-                           st->cf.inv_dt, st->V(2), s, gate));
-    const bool hf = st->has_frac;
-    CK(launch_pressure_general(st->g, st->cf, st->tb, st->P(), st->Pn(), st->V(0), st->V(1), st->V(2),
-                               hf ? st->d_frac[0] : nullptr, hf ? st->d_frac[1] : nullptr,
-                               hf ? st->d_frac[2] : nullptr, st->d_solid, s, gate));
-    st->launches += 3;
     st->cur ^= 1;
-    ++st->step_count;
-    const int trace0 = st->trace_len;
-    if (st->n_rec > 0 && st->trace_len < st->trace_cap) {
-        CK(launch_wsum(st->P(), st->d_rec_idx, st->d_rec_w, st->n_rec, 8, 0,
-                       st->d_trace + (size_t)st->trace_len * st->n_rec, s));
-        ++st->trace_len;
-        ++st->launches;
-    }
-    const bool checked = (st->step_count & (kCheckPeriod - 1)) == 0;
-    const int phase0 = st->stab_phase;
-    if (checked) {
-        st->stab_phase = (phase0 + 1) % kCheckStride;
-        CK(cudaMemsetAsync(st->d_status + kStatusCell, 0xFF, sizeof(unsigned), s));
-        CK(launch_check(st->g, st->P(), st->N, phase0, st->d_status, st->step_count, s, gate));
-        ++st->launches;
-    }
-    // saddle samples (taps staged by the caller) from the new displacement
-    if (n_saddle > 0) {
-        const size_t n = (size_t)n_saddle * 4;
-        if (int rc2 = upload_taps(st, n, s)) return rc2;
-        CK(launch_wsum(st->d_w[st->wi_cur], st->d_sidx, st->d_sw, n_saddle, 4, 0, st->d_sout, s));
-        ++st->launches;
-        CK(cudaMemcpyAsync(st->h_sout, st->d_sout, (size_t)n_saddle * sizeof(float), cudaMemcpyDeviceToHost, s));
-    }
-    CK(cudaMemcpyAsync(st->h_status, st->d_status, kStatusWords * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
+    st->step_count = step1;
+    if (record) ++st->trace_len;
+    if (checked) st->stab_phase = (phase0 + 1) % kCheckStride;
     CK(cudaStreamSynchronize(s));
 
     const unsigned bad = st->h_status[kStatusPlate];
