@@ -589,12 +589,19 @@ int flush_record(AcousticFDTDState* st)
 // by the next fused step's kernel from its input pressure; the caller ends
 // its run of steps with flush_record.  On the fused path the point-source
 // deposit of an open source cell is applied inside the step kernel too.
+int substep_plate(AcousticFDTDState* st, int n_saddle, float* out);
+
 int one_step(AcousticFDTDState* st, bool sync_check, bool defer_record = false)
 {
     cudaStream_t s = st->stream;
     const bool fused = use_fused(st);
     if (!fused) {
         if (int rc0 = flush_record(st)) return rc0;
+        // A plate scene on the two-pass kernels waits for its plate guard every
+        // step anyway: take the substep's schedule (all of the step issued, the
+        // guard read with the status words at its end, graph replay where it
+        // applies), which leaves the same state and return codes.
+        if (st->n_act > 0 && sync_check && !st->prof_on) return substep_plate(st, 0, nullptr);
     }
     // point source: deposit s[n] before step n (applies before the plate reads P)
     bool fuse_deposit = false;
