@@ -79,6 +79,7 @@ struct ProfEvents {
 struct SubstepKey {
     cudaStream_t stream;
     const float *p, *pn, *v0, *v1, *v2, *w_cur, *w_prev, *w_tmp, *frac[3], *ext, *h_ext;
+    const int2 *pack, *h_pack;
     const uint8_t* solid;
     const long long *sidx;
     const float *sw;
@@ -88,7 +89,7 @@ struct SubstepKey {
     Coef cf;
     Tables tb;
     PlateCoef pc;
-    int n_act, n_plate, n_saddle, ext_copy, ext_zero, has_frac;
+    int n_act, n_plate, n_saddle, ext_copy, ext_zero, has_frac, n_pack;
 };
 
 struct SubstepGraph {
@@ -148,6 +149,12 @@ struct AcousticFDTDState {
     float* h_ext = nullptr;          // pinned, N_plate: forces pending for the next step
     bool ext_pending = false;
     bool dev_ext_nonzero = false;
+    // plate nodes holding a pending force, each once, and their (node, value)
+    // pairs as the substep sends them (pinned) and as the device receives them
+    std::vector<int> ext_nodes;
+    std::vector<uint8_t> ext_mark;
+    int2* h_ext_pack = nullptr;
+    int2* d_ext_pack = nullptr;
 
     std::vector<int> src_idx;
     std::vector<float> src_wgt;
@@ -589,6 +596,26 @@ int flush_record(AcousticFDTDState* st)
 // by the next fused step's kernel from its input pressure; the caller ends
 // its run of steps with flush_record.  On the fused path the point-source
 // deposit of an open source cell is applied inside the step kernel too.
+// A plate node that receives a pending force (recorded once).
+inline void note_ext(AcousticFDTDState* st, int pidx)
+{
+    if (!st->ext_mark[pidx]) {
+        st->ext_mark[pidx] = 1;
+        st->ext_nodes.push_back(pidx);
+    }
+}
+
+// The pending forces consumed: their host entries (the only nonzero ones) back to zero.
+void clear_ext_host(AcousticFDTDState* st)
+{
+    for (int pidx : st->ext_nodes) {
+        st->h_ext[pidx] = 0.0f;
+        st->ext_mark[pidx] = 0;
+    }
+    st->ext_nodes.clear();
+    st->ext_pending = false;
+}
+
 int substep_plate(AcousticFDTDState* st, int n_saddle, float* out);
 
 int one_step(AcousticFDTDState* st, bool sync_check, bool defer_record = false)
@@ -645,17 +672,13 @@ int one_step(AcousticFDTDState* st, bool sync_check, bool defer_record = false)
             CK(cudaMemsetAsync(st->d_ext, 0, (size_t)st->N_plate * sizeof(float), s));
             st->dev_ext_nonzero = false;
         }
-        if (st->ext_pending) {
-            memset(st->h_ext, 0, (size_t)st->N_plate * sizeof(float));
-            st->ext_pending = false;
-        }
+        if (st->ext_pending) clear_ext_host(st);
         int t = st->wi_prev;
         st->wi_prev = st->wi_cur;
         st->wi_cur = st->wi_tmp;
         st->wi_tmp = t;
     } else if (st->ext_pending) {
-        memset(st->h_ext, 0, (size_t)st->N_plate * sizeof(float));   // consumed with no plate
-        st->ext_pending = false;
+        clear_ext_host(st);   // consumed with no plate
     }
 
     // velocity + pressure
@@ -784,6 +807,8 @@ void free_state(AcousticFDTDState* st)
     cudaFree(st->d_act); cudaFree(st->d_nb13); cudaFree(st->d_above); cudaFree(st->d_below);
     cudaFree(st->d_vzb); cudaFree(st->d_vza); cudaFree(st->d_pfix); cudaFree(st->d_ext); cudaFree(st->d_slice);
     cudaFreeHost(st->h_ext);
+    cudaFreeHost(st->h_ext_pack);
+    cudaFree(st->d_ext_pack);
     cudaFree(st->d_ps_sig);
     cudaFree(st->d_rec_idx); cudaFree(st->d_rec_w); cudaFree(st->d_trace);
     cudaFree(st->d_status); cudaFreeHost(st->h_status);
@@ -929,6 +954,9 @@ AcousticFDTDState* create_impl(int Nx, int Ny, int Nz, float dx, float c, float 
     CKN(cudaMemsetAsync(st->d_ext, 0, sizeof(float) * st->N_plate, st->stream));
     CKN(cudaMallocHost(&st->h_ext, sizeof(float) * st->N_plate));
     memset(st->h_ext, 0, sizeof(float) * st->N_plate);
+    st->ext_mark.assign((size_t)st->N_plate, 0);
+    CKN(cudaMallocHost(&st->h_ext_pack, sizeof(int2) * std::max(st->N_plate, 1)));
+    CKN(cudaMalloc(&st->d_ext_pack, sizeof(int2) * std::max(st->N_plate, 1)));
     {
         static const int DI[13] = {0, 1, -1, 0, 0, 1, 1, -1, -1, 2, -2, 0, 0};
         static const int DJ[13] = {0, 0, 0, 1, -1, 1, -1, 1, -1, 0, 0, 2, -2};
@@ -1054,6 +1082,7 @@ int fdtd_inject_bridge_drive(AcousticFDTDState* st, const float* cell_drives, fl
     for (size_t i = 0; i < st->src_idx.size(); ++i) {
         int pidx = st->src_idx[i] / st->Nz;
         if (pidx < 0 || pidx >= st->N_plate) return FDTD_ERR_ARG;
+        note_ext(st, pidx);
         st->h_ext[pidx] += force_scale * cell_drives[i] * inv_dx2;
     }
     st->ext_pending = true;
@@ -1070,6 +1099,7 @@ int fdtd_inject_plate_force(AcousticFDTDState* st, int n_plate, const int* plate
         int pidx = plate_indices[i];
         if (pidx < 0 || pidx >= st->N_plate) continue;
         if (!st->plate_active[pidx]) continue;
+        note_ext(st, pidx);
         st->h_ext[pidx] += total_force_N * weights[i] * inv_dx2;
         st->ext_pending = true;
     }
@@ -1194,8 +1224,7 @@ int fdtd_reset(AcousticFDTDState* st)
     CK(cudaMemsetAsync(st->d_status, 0xFF, kStatusWords * sizeof(unsigned), st->stream));
     CK(cudaStreamSynchronize(st->stream));
     for (int w = 0; w < kStatusWords; ++w) st->h_status[w] = 0xFFFFFFFFu;
-    memset(st->h_ext, 0, sizeof(float) * st->N_plate);
-    st->ext_pending = false;
+    clear_ext_host(st);
     st->dev_ext_nonzero = false;
     st->step_count = 0;
     st->trace_len = 0;
@@ -2000,8 +2029,18 @@ int substep_plate(AcousticFDTDState* st, int n_saddle, float* out)
         st->ps_done_step = st->step_count;
     }
     const bool ext_was_pending = st->ext_pending;
+    const bool ext_left = st->dev_ext_nonzero && !ext_was_pending;   // not expected; zeroed in full then
     if (st->ext_pending) st->dev_ext_nonzero = true;
     const bool ext_zero = st->dev_ext_nonzero;
+    // the pending forces as (node, value) pairs: only their nodes are nonzero on
+    // the host, and only they are written to (and later cleared on) the device
+    const int n_pack = ext_was_pending ? (int)st->ext_nodes.size() : 0;
+    for (int q = 0; q < n_pack; ++q) {
+        const int pidx = st->ext_nodes[q];
+        int bits;
+        memcpy(&bits, &st->h_ext[pidx], 4);
+        st->h_ext_pack[q] = make_int2(pidx, bits);
+    }
     if (n_saddle > 0)   // the saddle taps (staged by the caller) go up before the step's work
         if (int rc2 = upload_taps(st, (size_t)n_saddle * 4, s)) return rc2;
     const int wp0 = st->wi_prev, wc0 = st->wi_cur, wt0 = st->wi_tmp;
@@ -2019,12 +2058,15 @@ int substep_plate(AcousticFDTDState* st, int n_saddle, float* out)
     // plate's new displacement is d_w[wt0], the previous one d_w[wc0]), then
     // the saddle samples and the status words to the host.
     auto issue = [&]() -> int {
-        if (ext_was_pending)
-            CK(cudaMemcpyAsync(st->d_ext, st->h_ext, (size_t)st->N_plate * sizeof(float), cudaMemcpyHostToDevice, s));
+        if (n_pack > 0) {
+            CK(cudaMemcpyAsync(st->d_ext_pack, st->h_ext_pack, (size_t)n_pack * sizeof(int2), cudaMemcpyHostToDevice, s));
+            CK(launch_ext_scatter(st->d_ext, st->d_ext_pack, n_pack, s));
+        }
         CK(cudaMemsetAsync(st->d_status + kStatusPlate, 0xFF, sizeof(unsigned), s));
         CK(launch_plate_step(st->n_act, st->d_act, st->d_nb13, st->d_above, st->d_below, st->d_w[wc0], st->d_w[wp0],
                              st->d_w[wt0], st->d_ext, P, st->pc, st->d_status, s));
-        if (ext_zero) CK(launch_zero_gated(st->d_ext, st->N_plate, gate, s));
+        if (ext_left) CK(launch_zero_gated(st->d_ext, st->N_plate, gate, s));
+        else if (ext_zero) CK(launch_zero_gated_list(st->d_ext, st->d_ext_pack, n_pack, gate, s));
         CK(launch_velocity_general(st->g, st->cf, st->tb, P, st->V(0), st->V(1), st->V(2), st->d_frac[0],
                                    st->d_frac[1], st->d_frac[2], s, gate));
         CK(launch_plate_inject(st->n_act, st->d_act, st->d_vzb, st->d_vza, st->d_w[wt0], st->d_w[wc0], st->cf.inv_dt,
@@ -2046,7 +2088,8 @@ int substep_plate(AcousticFDTDState* st, int n_saddle, float* out)
         CK(cudaMemcpyAsync(st->h_status, st->d_status, kStatusWords * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
         return FDTD_OK;
     };
-    const long long n_launch = 4 + (ext_zero ? 1 : 0) + (record ? 1 : 0) + (checked ? 1 : 0) + (n_saddle > 0 ? 1 : 0);
+    const long long n_launch = 4 + (n_pack > 0 ? 1 : 0) + ((ext_left || (ext_zero && n_pack > 0)) ? 1 : 0) +
+                               (record ? 1 : 0) + (checked ? 1 : 0) + (n_saddle > 0 ? 1 : 0);
     bool issued = false;
     if (!record && !checked) {
         // The same work recurs every substep with one of a few pointer sets:
@@ -2058,6 +2101,7 @@ int substep_plate(AcousticFDTDState* st, int n_saddle, float* out)
         k.w_cur = st->d_w[wc0]; k.w_prev = st->d_w[wp0]; k.w_tmp = st->d_w[wt0];
         for (int c2 = 0; c2 < 3; ++c2) k.frac[c2] = st->d_frac[c2];
         k.ext = st->d_ext; k.h_ext = st->h_ext; k.solid = st->d_solid;
+        k.pack = st->d_ext_pack; k.h_pack = st->h_ext_pack; k.n_pack = n_pack;
         k.sidx = st->d_sidx; k.sw = st->d_sw; k.sout = st->d_sout; k.h_sout = st->h_sout;
         k.status = st->d_status; k.h_status = st->h_status;
         k.g = st->g; k.cf = st->cf; k.tb = st->tb; k.pc = st->pc;
@@ -2126,10 +2170,7 @@ int substep_plate(AcousticFDTDState* st, int n_saddle, float* out)
         return FDTD_ERR_UNSTABLE;   // pending forces stay, as after fdtd_step
     }
     st->dev_ext_nonzero = false;    // consumed by the gated zeroing
-    if (ext_was_pending) {
-        memset(st->h_ext, 0, (size_t)st->N_plate * sizeof(float));
-        st->ext_pending = false;
-    }
+    if (ext_was_pending) clear_ext_host(st);
     if (checked) {
         if (int rc2 = check_timeout(st)) return rc2;
         const unsigned cell = st->h_status[kStatusCell];
