@@ -480,7 +480,11 @@ FDTD_B200_API int fdtd_b200_slab_get_traces(FdtdB200Slab* h, float* out, int out
  * results and return codes as that sequence (the saddle indices are checked
  * before stepping) and one stream synchronisation instead of two: the plate
  * guard of the step is evaluated on the device and read back together with
- * the saddle samples.  out_saddle_w is written only when the step succeeds. */
+ * the saddle samples.  out_saddle_w is written only when the step succeeds.
+ * When the handle records no receivers on the device and the step takes no
+ * stability check, the device work is replayed from a cached CUDA graph
+ * (kept per set of buffers and flags, at most 12 per handle) on the handle's
+ * stream; on a stream that cannot be captured it is issued directly. */
 FDTD_B200_API int fdtd_b200_substep(AcousticFDTDState* st, const float* cell_drives,
                                     float drive_scale, int n_force, const int* force_idx,
                                     const float* force_wgt, float force_total_N, int n_saddle,

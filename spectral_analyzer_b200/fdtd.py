@@ -295,7 +295,9 @@ class AcousticFDTD:
         """One co-evolver substep in one call (fdtd_b200_substep): bridge drive,
         plate force, one step and the saddle samples, as inject_bridge_drive,
         inject_plate_force, step(1) and sample_plate_displacement_batch would
-        give them, with one stream synchronisation.  Returns the saddle samples."""
+        give them, with one stream synchronisation.  When no receivers are
+        recorded on the device, the substep's device work is replayed as a
+        cached CUDA graph.  Returns the saddle samples."""
         drv = _f32(cell_drives) if cell_drives is not None else None
         fi = _i32(force_idx if force_idx is not None else [])
         fw = _f32(force_wgt if force_wgt is not None else np.zeros(fi.size), fi.size)
