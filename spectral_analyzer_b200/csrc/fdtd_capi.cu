@@ -137,6 +137,7 @@ struct AcousticFDTDState {
     long long* d_below = nullptr;
     long long* d_vzb = nullptr;
     long long* d_vza = nullptr;
+    uint8_t* d_plate_code = nullptr;   // per plate node: bit 0 Vz face below, bit 1 above (PlateFaces)
     // four-cell groups whose divergence reads a plate face (padded index of the
     // group's first cell): recomputed after a walled single-pass step
     long long* d_pfix = nullptr;
@@ -735,18 +736,23 @@ int one_step(AcousticFDTDState* st, bool sync_check, bool defer_record = false)
         }
         if ((rc = prof_end(st, e1, fused_kernel_launches_per_step()))) return rc;
     } else {
+        PlateFaces pf;   // the plate's face velocities, set inside the velocity pass
+        if (st->n_act > 0) {
+            pf.code = st->d_plate_code;
+            pf.w = st->d_w[st->wi_cur];
+            pf.wp = st->d_w[st->wi_prev];
+            pf.inv_dt = st->cf.inv_dt;
+            pf.iz = st->plate_iz;
+        }
         CK(launch_velocity_general(st->g, st->cf, st->tb, st->P(), st->V(0), st->V(1), st->V(2),
-                                   st->d_frac[0], st->d_frac[1], st->d_frac[2], s));
-        st->launches += 2 + (st->n_act > 0 ? 1 : 0);
-        if (st->n_act > 0)
-            CK(launch_plate_inject(st->n_act, st->d_act, st->d_vzb, st->d_vza, st->d_w[st->wi_cur],
-                                   st->d_w[st->wi_prev], st->cf.inv_dt, st->V(2), s));
+                                   st->d_frac[0], st->d_frac[1], st->d_frac[2], s, nullptr, &pf));
+        st->launches += 2;
         const bool hf = st->has_frac;
         CK(launch_pressure_general(st->g, st->cf, st->tb, st->P(), st->Pn(), st->V(0), st->V(1),
                                    st->V(2), hf ? st->d_frac[0] : nullptr,
                                    hf ? st->d_frac[1] : nullptr, hf ? st->d_frac[2] : nullptr,
                                    st->d_solid, s));
-        if ((rc = prof_end(st, e1, st->n_act > 0 ? 3 : 2))) return rc;
+        if ((rc = prof_end(st, e1, 2))) return rc;
     }
     st->cur ^= 1;
     ++st->step_count;
@@ -805,7 +811,7 @@ void free_state(AcousticFDTDState* st)
     cudaFree(st->d_solid);
     for (int c = 0; c < 3; ++c) { cudaFree(st->d_frac[c]); cudaFree(st->d_w[c]); }
     cudaFree(st->d_act); cudaFree(st->d_nb13); cudaFree(st->d_above); cudaFree(st->d_below);
-    cudaFree(st->d_vzb); cudaFree(st->d_vza); cudaFree(st->d_pfix); cudaFree(st->d_ext); cudaFree(st->d_slice);
+    cudaFree(st->d_vzb); cudaFree(st->d_vza); cudaFree(st->d_pfix); cudaFree(st->d_plate_code); cudaFree(st->d_ext); cudaFree(st->d_slice);
     cudaFreeHost(st->h_ext);
     cudaFreeHost(st->h_ext_pack);
     cudaFree(st->d_ext_pack);
@@ -997,6 +1003,11 @@ AcousticFDTDState* create_impl(int Nx, int Ny, int Nz, float dx, float c, float 
             CKN(cudaMemcpy(st->d_below, below.data(), na * sizeof(long long), cudaMemcpyHostToDevice));
             CKN(cudaMemcpy(st->d_vzb, vzb.data(), na * sizeof(long long), cudaMemcpyHostToDevice));
             CKN(cudaMemcpy(st->d_vza, vza.data(), na * sizeof(long long), cudaMemcpyHostToDevice));
+            std::vector<uint8_t> code((size_t)st->N_plate, 0);
+            for (size_t q = 0; q < na; ++q)
+                code[st->h_act[q]] = (uint8_t)((vzb[q] >= 0 ? 1 : 0) | (vza[q] >= 0 ? 2 : 0));
+            CKN(cudaMalloc(&st->d_plate_code, code.size()));
+            CKN(cudaMemcpy(st->d_plate_code, code.data(), code.size(), cudaMemcpyHostToDevice));
             // cells whose pressure update reads plate face kf: k = kf-1 .. kf+2
             std::vector<long long> fix;
             for (const auto* lst : {&vzb, &vza})
@@ -2066,11 +2077,19 @@ int substep_plate(AcousticFDTDState* st, int n_saddle, float* out)
         CK(launch_plate_step(st->n_act, st->d_act, st->d_nb13, st->d_above, st->d_below, st->d_w[wc0], st->d_w[wp0],
                              st->d_w[wt0], st->d_ext, P, st->pc, st->d_status, s));
         if (ext_left) CK(launch_zero_gated(st->d_ext, st->N_plate, gate, s));
-        else if (ext_zero) CK(launch_zero_gated_list(st->d_ext, st->d_ext_pack, n_pack, gate, s));
+        PlateFaces pf;   // plate face velocities and the consumed forces' zeroing, in the velocity pass
+        pf.code = st->d_plate_code;
+        pf.w = st->d_w[wt0];
+        pf.wp = st->d_w[wc0];
+        pf.inv_dt = st->cf.inv_dt;
+        pf.iz = st->plate_iz;
+        if (!ext_left && ext_zero) {
+            pf.ext = st->d_ext;
+            pf.pack = st->d_ext_pack;
+            pf.m = n_pack;
+        }
         CK(launch_velocity_general(st->g, st->cf, st->tb, P, st->V(0), st->V(1), st->V(2), st->d_frac[0],
-                                   st->d_frac[1], st->d_frac[2], s, gate));
-        CK(launch_plate_inject(st->n_act, st->d_act, st->d_vzb, st->d_vza, st->d_w[wt0], st->d_w[wc0], st->cf.inv_dt,
-                               st->V(2), s, gate));
+                                   st->d_frac[1], st->d_frac[2], s, gate, &pf));
         CK(launch_pressure_general(st->g, st->cf, st->tb, P, Pn, st->V(0), st->V(1), st->V(2),
                                    hf ? st->d_frac[0] : nullptr, hf ? st->d_frac[1] : nullptr,
                                    hf ? st->d_frac[2] : nullptr, st->d_solid, s, gate));
@@ -2088,8 +2107,8 @@ int substep_plate(AcousticFDTDState* st, int n_saddle, float* out)
         CK(cudaMemcpyAsync(st->h_status, st->d_status, kStatusWords * sizeof(unsigned), cudaMemcpyDeviceToHost, s));
         return FDTD_OK;
     };
-    const long long n_launch = 4 + (n_pack > 0 ? 1 : 0) + ((ext_left || (ext_zero && n_pack > 0)) ? 1 : 0) +
-                               (record ? 1 : 0) + (checked ? 1 : 0) + (n_saddle > 0 ? 1 : 0);
+    const long long n_launch = 3 + (n_pack > 0 ? 1 : 0) + (ext_left ? 1 : 0) + (record ? 1 : 0) + (checked ? 1 : 0) +
+                               (n_saddle > 0 ? 1 : 0);
     bool issued = false;
     if (!record && !checked) {
         // The same work recurs every substep with one of a few pointer sets:

@@ -50,10 +50,13 @@ __device__ __forceinline__ void unpack(const float4& x, float (&v)[4]) { v[0] = 
 __global__ void __launch_bounds__(256) k_velocity_general(
     Grid g, Coef cf, Tables tb, const float* __restrict__ p, float* __restrict__ vx,
     float* __restrict__ vy, float* __restrict__ vz, const float* __restrict__ fx,
-    const float* __restrict__ fy, const float* __restrict__ fz, const unsigned* __restrict__ gate)
+    const float* __restrict__ fy, const float* __restrict__ fz, const unsigned* __restrict__ gate,
+    PlateFaces pf)
 {
-    GEN_INDEX
     if (gate && gate[kStatusPlate] != 0xFFFFFFFFu) return;   // this step's plate update failed
+    if (pf.m > 0 && blockIdx.x == 0 && blockIdx.y == 0)      // the consumed plate forces
+        for (int q = threadIdx.x; q < pf.m; q += blockDim.x) pf.ext[pf.pack[q].x] = 0.0f;
+    GEN_INDEX
     const float ay = __ldg(tb.ay + j), axi = __ldg(tb.ax + i);
     float pc[4], az4[4], ac[4];
     unpack(ld4(p, id), pc);
@@ -127,6 +130,16 @@ __global__ void __launch_bounds__(256) k_velocity_general(
                             face_damp(ac[q], fmaxf(fmaxf(axi, ay), __ldg(tb.az + k + 1)), cf.dt));
             if (fz && fr[q] == 0.0f) nv = 0.0f;
             v[q] = nv;
+        }
+        if (pf.code && k0 <= pf.iz && pf.iz - 1 <= k0 + 3) {   // the plate's faces
+            const int node = j + g.ny * i;
+            const unsigned c = pf.code[node];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                const int k = k0 + q;
+                if ((k == pf.iz - 1 && (c & 1u)) || (k == pf.iz && (c & 2u)))
+                    v[q] = fmul(fsub(pf.w[node], pf.wp[node]), pf.inv_dt);
+            }
         }
         st4(vz, id, v);
     }
@@ -367,11 +380,12 @@ __global__ void k_slice(const float* __restrict__ f, Grid g, int axis, int idx, 
 cudaError_t launch_velocity_general(const Grid& g, const Coef& cf, const Tables& tb,
                                     const float* p, float* vx, float* vy, float* vz,
                                     const float* fx, const float* fy, const float* fz,
-                                    cudaStream_t s, const unsigned* gate)
+                                    cudaStream_t s, const unsigned* gate, const PlateFaces* pf)
 {
     dim3 block(256, 1, 1);
     dim3 grid((g.ny * ((g.nz + 3) / 4) + 255) / 256, g.nx, 1);
-    k_velocity_general<<<grid, block, 0, s>>>(g, cf, tb, p, vx, vy, vz, fx, fy, fz, gate);
+    k_velocity_general<<<grid, block, 0, s>>>(g, cf, tb, p, vx, vy, vz, fx, fy, fz, gate,
+                                              pf ? *pf : PlateFaces());
     return cudaGetLastError();
 }
 

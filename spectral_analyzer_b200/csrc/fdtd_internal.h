@@ -80,6 +80,23 @@ struct PlateCoef {
     float bk;   // beta_K / dt * bh
 };
 
+// Extra jobs of the two-pass velocity pass for a plate scene (code null: none):
+// the plate's face velocities (w - w_prev)/dt on the Vz faces below (code bit 0)
+// and above (bit 1) each active node, which overwrite the updated faces as
+// k_plate_inject does; and, by the first block, the entries of the consumed
+// plate forces back to zero (pack/m, m = 0: none).  Both are skipped when the
+// gate reports a failed plate update.
+struct PlateFaces {
+    const uint8_t* code = nullptr;   // [Nx * Ny], node j + Ny * i
+    const float* w = nullptr;
+    const float* wp = nullptr;
+    float inv_dt = 0.0f;
+    int iz = -1;
+    float* ext = nullptr;
+    const int2* pack = nullptr;
+    int m = 0;
+};
+
 // Targets of one pressure deposit (deposit_pressure_open, acoustic_fdtd.cpp:840-872):
 // divisor 0 = add the amplitude to idx[0]; divisor m > 0 = add amp/m to idx[0..n).
 struct Deposit {
@@ -129,7 +146,8 @@ __device__ __forceinline__ float sample8(const float* f, const long long* idx, c
 cudaError_t launch_velocity_general(const Grid& g, const Coef& cf, const Tables& tb,
                                     const float* p, float* vx, float* vy, float* vz,
                                     const float* fx, const float* fy, const float* fz,
-                                    cudaStream_t s, const unsigned* gate = nullptr);
+                                    cudaStream_t s, const unsigned* gate = nullptr,
+                                    const PlateFaces* pf = nullptr);
 // pressure update of listed four-cell groups (plate-face neighbours after a walled single-pass step)
 cudaError_t launch_pressure_groups(const Grid& g, const Coef& cf, const Tables& tb, const float* p, float* pn,
                                    const float* vx, const float* vy, const float* vz, const float* fx,
