@@ -353,15 +353,6 @@ __global__ void k_ext_scatter(float* __restrict__ ext, const int2* __restrict__ 
     if (q < m) ext[pack[q].x] = __int_as_float(pack[q].y);
 }
 
-// After a plate update that succeeded: the entries the forces occupied back to zero.
-__global__ void k_zero_gated_list(float* __restrict__ ext, const int2* __restrict__ pack, int m,
-                                  const unsigned* __restrict__ gate)
-{
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
-    if (q >= m || gate[kStatusPlate] != 0xFFFFFFFFu) return;
-    ext[pack[q].x] = 0.0f;
-}
-
 // One plane of a field across the given axis, rows of the remaining two axes
 // in (i, j, k) order: axis 0 -> (Ny, Nz), 1 -> (Nx, Nz), 2 -> (Nx, Ny).
 __global__ void k_slice(const float* __restrict__ f, Grid g, int axis, int idx, float* __restrict__ out,
@@ -468,13 +459,6 @@ cudaError_t launch_ext_scatter(float* ext, const int2* pack, int m, cudaStream_t
 {
     if (m <= 0) return cudaSuccess;
     k_ext_scatter<<<(m + 255) / 256, 256, 0, s>>>(ext, pack, m);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_zero_gated_list(float* ext, const int2* pack, int m, const unsigned* gate, cudaStream_t s)
-{
-    if (m <= 0) return cudaSuccess;
-    k_zero_gated_list<<<(m + 255) / 256, 256, 0, s>>>(ext, pack, m, gate);
     return cudaGetLastError();
 }
 

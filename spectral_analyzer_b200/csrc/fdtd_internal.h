@@ -162,10 +162,9 @@ cudaError_t launch_plate_step(int n_act, const int* act, const int* nb13, const 
                               const long long* below, const float* w, const float* wp, float* wt,
                               const float* ext, const float* p, const PlateCoef& pc,
                               unsigned* status, cudaStream_t s);
-// plate forces as (node, value) pairs: scatter into the zeroed device buffer,
-// and the gated return of those entries to zero after the plate update
+// plate forces as (node, value) pairs scattered into the zeroed device buffer
+// (the velocity pass returns them to zero: PlateFaces)
 cudaError_t launch_ext_scatter(float* ext, const int2* pack, int m, cudaStream_t s);
-cudaError_t launch_zero_gated_list(float* ext, const int2* pack, int m, const unsigned* gate, cudaStream_t s);
 cudaError_t launch_plate_inject(int n_act, const int* act, const long long* vzb,
                                 const long long* vza, const float* w, const float* wp,
                                 float inv_dt, float* vz, cudaStream_t s,
