@@ -75,7 +75,11 @@ struct H16 {
     static_assert(PC <= 256 && PR <= 256, "TMA box extent");
 };
 
-constexpr int kD16 = 2;
+// Prefetch distance (planes): 3 for the plain 16-bit forms (same box:
+// BF16 146.2 -> 146.8, FP16 136.6 -> 138.5 Gcell/s against 2); 2 for the
+// compensated forms, whose boxes at 3 leave one CTA per SM (half the rate).
+template <int M>
+__host__ __device__ constexpr int depth16() { return Traits<M>::comp ? 2 : 3; }
 
 // Exact decode / encode of the stored forms (as ld4 / st4 of the two-pass
 // kernels); the residual arguments are ignored by the plain 16-bit forms.
@@ -211,7 +215,7 @@ template <int M>
 __global__ void __launch_bounds__(256) k_fused16(F16Args a, const __grid_constant__ Maps16 mp, int seg_len,
                                                   int tiles_k)
 {
-    using C = H16<M, kD16>;
+    using C = H16<M, depth16<M>()>;
     using K = Code<M>;
     const Grid g = a.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz, sz = g.sz;
@@ -606,7 +610,7 @@ std::mutex g_cfg16_mu;
 template <int M>
 cudaError_t launch_of(const F16Args& a, F16Cache* cache, const void* const bases[8], cudaStream_t s)
 {
-    using C = H16<M, kD16>;
+    using C = H16<M, depth16<M>()>;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
@@ -686,10 +690,10 @@ bool f16_supported(int mode, const Grid& g)
 size_t f16_smem_bytes(int mode)
 {
     switch (mode) {
-        case kBF16: return H16<kBF16, kD16>::SMEM_BYTES;
-        case kFP16: return H16<kFP16, kD16>::SMEM_BYTES;
-        case kBF16C: return H16<kBF16C, kD16>::SMEM_BYTES;
-        case kFP16C: return H16<kFP16C, kD16>::SMEM_BYTES;
+        case kBF16: return H16<kBF16, depth16<kBF16>()>::SMEM_BYTES;
+        case kFP16: return H16<kFP16, depth16<kFP16>()>::SMEM_BYTES;
+        case kBF16C: return H16<kBF16C, depth16<kBF16C>()>::SMEM_BYTES;
+        case kFP16C: return H16<kFP16C, depth16<kFP16C>()>::SMEM_BYTES;
         default: return 0;
     }
 }
